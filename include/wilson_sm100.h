@@ -1,0 +1,172 @@
+/*
+ * wilson_sm100.h -- C-ABI of libwilson_sm100.so, the sm_100a (B200) SU(3)
+ * Wilson-fermion hot path: Dirac operator D, D^dag, even-odd Schur blocks,
+ * mixed-precision multi-RHS CG, and the Nf=2 pseudofermion force.
+ *
+ * Conventions (identical to jaxQFT's):
+ *   - gauge field: one configuration, complex128 interleaved, layout BMXYIJ
+ *     [mu=4][Lx][Ly][Lz][Lt][3][3]  (jaxqft/models/su3_ym.py:246-249)
+ *   - fermion field: complex128 [nrhs][Lx][Ly][Lz][Lt][Ns=4][Nc=3], t fastest
+ *     (jaxqft/models/su3_wilson_nf2.py:815-817)
+ *   - D = (m + 4r) - 1/2 sum_mu [(r - g_mu) U_mu(x) psi(x+mu) + (r + g_mu) U_mu^dag(x-mu) psi(x-mu)]
+ *     with the Euclidean gammas of jaxqft/fermions/gamma.py:14-46, r = 1
+ *   - boundary phase bc[mu] multiplies U_mu(x) on x_mu = L_mu - 1
+ *     (jaxqft/models/su3_wilson_nf2.py:726-759)
+ * All field pointers are DEVICE pointers owned by the caller.  Every call is
+ * asynchronous on the context's stream unless stated otherwise.  A context is
+ * not thread-safe: callers serialise calls on one context.  No C++ exception
+ * crosses this boundary; every call returns a wl_status and, on failure,
+ * wl_last_error() describes it.
+ */
+#ifndef WILSON_SM100_H
+#define WILSON_SM100_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  WL_OK = 0,
+  WL_ERR_ARG = 1,         /* invalid argument (shape, parity, op, null pointer) */
+  WL_ERR_OOM = 2,         /* device allocation failed / HBM budget exceeded */
+  WL_NOT_CONVERGED = 3,   /* a solve stopped at maxiter (per-RHS status says which) */
+  WL_ERR_NAN = 4,         /* a solve produced a non-finite residual */
+  WL_ERR_TIMEOUT = 5,     /* a bounded device wait ran out */
+  WL_ERR_CUDA = 6,        /* CUDA runtime error */
+  WL_ERR_STATE = 7        /* call not valid in the current state */
+} wl_status;
+
+typedef enum { WL_PREC_DOUBLE = 0, WL_PREC_SINGLE = 1, WL_PREC_HALF = 2 } wl_prec;
+
+typedef enum {
+  /* full-lattice operators (jaxqft/models/su3_wilson_nf2.py:1036-1055, 1101-1105) */
+  WL_OP_D = 0,          /* apply_D */
+  WL_OP_DDAG = 1,       /* apply_Ddag */
+  WL_OP_DDAGD = 2,      /* apply_normal: D^dag (D psi) */
+  WL_OP_HOP = 3,        /* apply_offdiag: K = D - m0 */
+  WL_OP_HOP_DAG = 4,    /* apply_offdiag_dagger */
+  /* masked even/odd blocks on full-lattice fields (1057-1099): input projected
+     to the source parity, output zero on the other parity */
+  WL_OP_K_OE = 5,       /* apply_K_oe  (even -> odd) */
+  WL_OP_K_EO = 6,       /* apply_K_eo  (odd -> even) */
+  WL_OP_KDAG_OE = 7,    /* apply_Kdag_oe */
+  WL_OP_KDAG_EO = 8,    /* apply_Kdag_eo */
+  /* Schur complements (1112-1155): S_e = m0 - (1/m0) K_eo K_oe, normalized = S_e / m0 */
+  WL_OP_SCHUR_E = 9,      /* apply_eo_schur_even */
+  WL_OP_SCHUR_E_DAG = 10, /* apply_eo_schur_even_dagger */
+  WL_OP_SCHUR_O = 11,     /* apply_eo_schur_odd */
+  WL_OP_SCHUR_E_NORMAL = 12 /* S_e^dag S_e (the operator solve_eop_even_normal inverts) */
+} wl_op;
+
+#define WL_FLAG_NORMALIZED 1u
+
+typedef struct {
+  int dims[4];        /* Lx, Ly, Lz, Lt; all even */
+  double bc_re[4];    /* boundary phase per direction */
+  double bc_im[4];
+} wl_geometry;
+
+typedef struct wl_ctx wl_ctx;
+typedef struct wl_gauge wl_gauge;
+typedef struct wl_engine wl_engine;
+
+/* Library / context ------------------------------------------------------ */
+int wl_version(void);
+/* Create a context for one lattice geometry on CUDA device `device`.
+   Replaces the geometry set-up of SU3WilsonNf2.__post_init__
+   (jaxqft/models/su3_wilson_nf2.py:657-709: BC factor, masks, EO maps). */
+wl_status wl_ctx_create(const wl_geometry* geom, int device, wl_ctx** out);
+void wl_ctx_destroy(wl_ctx* ctx);
+const char* wl_last_error(const wl_ctx* ctx);
+/* Use `stream` (a cudaStream_t; NULL = legacy default) for subsequent calls. */
+wl_status wl_ctx_set_stream(wl_ctx* ctx, void* stream);
+wl_status wl_ctx_synchronize(wl_ctx* ctx);
+
+/* Even/odd index maps for bit-exact checks (su3_wilson_nf2.py:831-882):
+   even[Vh], odd[Vh] ascending flat indices; nbr[8][2][Vh] = compact index of
+   the opposite-parity neighbour x+mu (dir 0) / x-mu (dir 1) of compact site k
+   of parity p, laid out [p*4+mu][dir][k].  Host pointers, synchronous. */
+wl_status wl_eo_maps(wl_ctx* ctx, int32_t* even, int32_t* odd, int32_t* nbr);
+
+/* Gauge field ------------------------------------------------------------ */
+/* Build the internal parity-split FP64 (18- and 12-real), FP32 and FP16
+   12-real copies of one configuration.  Replaces _links_with_fermion_bc
+   (su3_wilson_nf2.py:751-759), which the kernels apply by index instead.
+   `U` stays owned by the caller and is not referenced after the call. */
+wl_status wl_gauge_create(wl_ctx* ctx, const void* U, wl_gauge** out);
+wl_status wl_gauge_update(wl_gauge* gauge, const void* U);
+/* max over links of |U U^dag - 1| and |det U - 1| (synchronous) */
+wl_status wl_gauge_unitarity(wl_gauge* gauge, double* err);
+void wl_gauge_destroy(wl_gauge* gauge);
+
+/* Operators on reference-layout fields, FP64 ----------------------------- */
+/* out = op(in) for nrhs fields.  `mass` is the bare mass m (m0 = m + 4).
+   `flags`: WL_FLAG_NORMALIZED for the Schur ops.  in and out must not alias. */
+wl_status wl_apply(wl_ctx* ctx, wl_gauge* gauge, int op, double mass, unsigned flags,
+                   const void* in, void* out, int nrhs);
+
+/* Solver ------------------------------------------------------------------ */
+typedef enum {
+  WL_SOLVE_NORMAL = 0,    /* (D^dag D) x = b on the full lattice: solve_normal (1410-1432) */
+  WL_SOLVE_EO_NORMAL = 1  /* (M^dag M) x_e = b_e, M = normalized even Schur:
+                             solve_eop_even_normal (1370-1392) */
+} wl_solve_op;
+
+typedef struct {
+  int op;            /* wl_solve_op */
+  int inner_prec;    /* wl_prec of the iterated operator; FP64 = plain CG */
+  double tol;        /* stop when ||b - A x|| <= tol ||b|| with A in FP64 */
+  int maxiter;
+  double delta;      /* reliable-update trigger: sloppy ||r|| < delta * max ||r|| since update */
+  int use_x0;        /* x holds an initial guess on entry */
+  int use_graph;     /* capture each CG iteration in a CUDA graph */
+  int check_every;   /* iterations between host convergence polls (0 = default) */
+} wl_solve_params;
+
+typedef struct {
+  int iters;            /* CG iterations */
+  int reliable_updates; /* FP64 true-residual recomputations */
+  int status;           /* 2 converged, 3 maxiter, 4 breakdown, 5 nan */
+  double true_res;      /* ||b - A x|| / ||b|| in FP64 at exit */
+} wl_solve_stats;
+
+/* Solve nrhs independent systems sharing the gauge field, one batched CG
+   (links streamed once per iteration for all RHS, converged RHS masked).
+   b, x: reference-layout fields.  `masses` holds one bare mass per RHS.
+   For WL_SOLVE_EO_NORMAL the odd sites of b are ignored and x is zero there,
+   as the reference's _unpack_even_sites does.  Synchronous (returns when all
+   RHS have stopped).  Replaces _solve_linear + jax.scipy.sparse.linalg.cg
+   (su3_wilson_nf2.py:1243-1269) for the cg/normal forms. */
+wl_status wl_solve(wl_ctx* ctx, wl_gauge* gauge, const wl_solve_params* params, const double* masses,
+                   const void* b, void* x, int nrhs, wl_solve_stats* stats);
+
+/* Continuous-batching engine: a fixed set of RHS slots that iterate together;
+   a slot can be admitted while others are mid-solve and retired when done. */
+wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* gauge, const wl_solve_params* params, int nslots,
+                           wl_engine** out);
+void wl_engine_destroy(wl_engine* eng);
+/* Admit `n` RHS into slots[0..n) (b: n consecutive reference-layout fields). */
+wl_status wl_engine_admit(wl_engine* eng, const int* slots, int n, const void* b, const double* masses,
+                          const double* tols, const int* maxiters);
+/* Run `iters` iterations on all active slots (asynchronous). */
+wl_status wl_engine_step(wl_engine* eng, int iters);
+/* Synchronise and report per-slot status (0 idle, 1 running, 2..5 stopped). */
+wl_status wl_engine_poll(wl_engine* eng, int* status, int* n_active);
+/* Copy the solution of slot `slot` into x (reference layout) and free the slot. */
+wl_status wl_engine_retire(wl_engine* eng, int slot, void* x, wl_solve_stats* stats);
+/* Size in bytes of the engine's device allocations (for HBM admission). */
+int64_t wl_engine_bytes(const wl_ctx* ctx, int op, int inner_prec, int nslots);
+
+/* Pseudofermion force ----------------------------------------------------- */
+/* F = pseudofermion_force_from_solution(U, X, Y) (su3_wilson_nf2.py:1556-1576):
+   F[mu][x] = TA( (c1 - c2)^T ), link-shaped complex128 BMXYIJ.  If
+   `accumulate` is non-zero, F += coef * force, else F = coef * force. */
+wl_status wl_pf_force(wl_ctx* ctx, wl_gauge* gauge, const void* X, const void* Y, double coef,
+                      int accumulate, void* F);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WILSON_SM100_H */

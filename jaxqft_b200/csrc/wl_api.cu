@@ -1,0 +1,1309 @@
+// libwilson_sm100: C-ABI implementation (contexts, gauge fields, operators,
+// batched mixed-precision CG engine, pseudofermion force).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdlib>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/wilson_sm100.h"
+#include "wl_force.cuh"
+#include "wl_site.cuh"
+
+using namespace wl;
+
+// ============================================================== error helpers
+struct wl_ctx {
+  Geom g;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // scratch for reference-layout operator chains (temp full fields)
+  void* tmp = nullptr;
+  size_t tmp_bytes = 0;
+};
+
+struct wl_gauge {
+  wl_ctx* ctx = nullptr;
+  double2* d18 = nullptr;
+  double2* d12 = nullptr;
+  float4* s12 = nullptr;
+  uint2* h12 = nullptr;
+  const double2* ref = nullptr;  // caller's reference-layout links (valid during wl_gauge_create/update only)
+  double2* ref_copy = nullptr;   // library-owned copy of the reference layout (for reference-layout kernels)
+  unsigned int* uerr = nullptr;  // device float bits
+  float unitarity = 0.f;
+  unsigned long long id = 0;     // unique per gauge object (graphs capture its buffers)
+};
+static std::atomic<unsigned long long> g_gauge_ids{1};
+extern "C" void wl_release_solve_cache(wl_ctx* ctx);
+
+static thread_local std::string g_static_err;
+
+static inline void set_err(wl_ctx* ctx, const std::string& m);
+#define WL_FAIL(ctx, code, msg) \
+  do {                          \
+    set_err((ctx), (msg));      \
+    return (code);              \
+  } while (0)
+
+#define WL_CUDA(ctx, call)                                                                          \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess) {                                                                        \
+      set_err((ctx), std::string(#call) + ": " + cudaGetErrorString(e_));                         \
+      return (e_ == cudaErrorMemoryAllocation) ? WL_ERR_OOM : WL_ERR_CUDA;                          \
+    }                                                                                               \
+  } while (0)
+
+static inline void set_err(wl_ctx* ctx, const std::string& m) {
+  if (ctx) ctx->err = m;
+  else g_static_err = m;
+}
+
+static wl_status check_launch(wl_ctx* ctx, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    ctx->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return WL_ERR_CUDA;
+  }
+  return WL_OK;
+}
+
+// ============================================================== field helpers
+static inline long long chunks_of(int prec) { return prec == P_DOUBLE ? 12 : (prec == P_SINGLE ? 6 : 3); }
+static inline size_t chunk_bytes() { return 16; }
+// bytes of one parity-half of one RHS (data + norm)
+static inline size_t half_bytes(int prec, int vh) {
+  return (size_t)chunks_of(prec) * chunk_bytes() * vh + (prec == P_HALF ? (size_t)vh * sizeof(float) : 0);
+}
+
+// A device field in the internal layout: nrhs x nparity halves, norms stored
+// after all data for FP16.
+struct IField {
+  void* data = nullptr;
+  float* norm = nullptr;
+  int prec = 0, vh = 0, nrhs = 0, npar = 1;
+  long long rstride() const { return chunks_of(prec) * vh * npar; }  // chunk elements per rhs
+};
+
+template <int P>
+static SpinorField<P> sf(const IField& f, int par) {
+  SpinorField<P> s;
+  using Ptr = decltype(s.ptr);
+  s.ptr = reinterpret_cast<Ptr>(f.data) + (long long)par * chunks_of(P) * f.vh;
+  s.norm = f.norm ? f.norm + (long long)par * f.vh : nullptr;
+  s.rstride = f.rstride();
+  s.vh = f.vh;
+  return s;
+}
+// field pair indexed by parity; for single-parity fields both entries alias par 0
+template <int P>
+static void sf2(const IField& f, SpinorField<P> (&o)[2]) {
+  o[0] = sf<P>(f, 0);
+  o[1] = f.npar == 2 ? sf<P>(f, 1) : o[0];
+}
+
+// FP16 norm layout with npar==2: norm index rhs*vh + c must land in [rhs][par][vh]:
+// handled by giving each parity its own base and a norm stride of npar*vh.
+// To keep SpinorField simple, FP16 norms use stride vh per rhs within a parity
+// block: norm[(par * nrhs + rhs) * vh + c].
+template <>
+SpinorField<P_HALF> sf<P_HALF>(const IField& f, int par) {
+  SpinorField<P_HALF> s;
+  s.ptr = reinterpret_cast<uint4*>(f.data) + (long long)par * 3 * f.vh;
+  s.norm = f.norm + (long long)par * f.nrhs * f.vh;
+  s.rstride = f.rstride();
+  s.vh = f.vh;
+  return s;
+}
+
+static wl_status alloc_field(wl_ctx* ctx, IField& f, int prec, int vh, int nrhs, int npar) {
+  f.prec = prec;
+  f.vh = vh;
+  f.nrhs = nrhs;
+  f.npar = npar;
+  size_t data = (size_t)chunks_of(prec) * 16 * vh * npar * nrhs;
+  size_t nb = data + (prec == P_HALF ? (size_t)vh * npar * nrhs * sizeof(float) : 0);
+  WL_CUDA(ctx, cudaMalloc(&f.data, nb));
+  WL_CUDA(ctx, cudaMemsetAsync(f.data, 0, nb, ctx->stream));
+  f.norm = prec == P_HALF ? reinterpret_cast<float*>(reinterpret_cast<char*>(f.data) + data) : nullptr;
+  return WL_OK;
+}
+static size_t field_bytes(int prec, int vh, int nrhs, int npar) {
+  size_t data = (size_t)chunks_of(prec) * 16 * vh * npar * nrhs;
+  return data + (prec == P_HALF ? (size_t)vh * npar * nrhs * sizeof(float) : 0);
+}
+static void free_field(IField& f) {
+  if (f.data) cudaFree(f.data);
+  f.data = nullptr;
+  f.norm = nullptr;
+}
+
+static SpinorRef sref(const void* p, const Geom& g) {
+  SpinorRef r;
+  r.ptr = (double2*)p;
+  r.rstride = 12LL * g.V;
+  r.Lt = g.L[3];
+  return r;
+}
+
+// ============================================================== launch helpers
+struct Tune {
+  int nr = 1, bx = 128, by = 1;
+};
+
+static dim3 grid_for(const Geom& g, const Tune& t, int nrhs, int npar) {
+  int groups = (nrhs + t.nr - 1) / t.nr;
+  return dim3((g.Vh + t.bx - 1) / t.bx, (groups + t.by - 1) / t.by, npar);
+}
+
+template <bool DAG, class IDX, class LF, class SF, class EPI>
+static void launch_hop(const Tune& t, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st) {
+  dim3 grid = grid_for(a.g, t, a.nrhs, npar), block(t.bx, t.by, 1);
+  switch (t.nr) {
+    case 4: hop_kernel<DAG, 4, IDX><<<grid, block, 0, st>>>(a); break;
+    case 2: hop_kernel<DAG, 2, IDX><<<grid, block, 0, st>>>(a); break;
+    default: hop_kernel<DAG, 1, IDX><<<grid, block, 0, st>>>(a); break;
+  }
+}
+
+template <class F>
+static void launch_site(const Tune& t, const Geom& g, int parity0, int npar, int nrhs, const int* mask, const F& f,
+                        Reduce red, cudaStream_t st) {
+  SiteArgs<F> a;
+  a.vh = g.Vh;
+  a.parity0 = parity0;
+  a.nrhs = nrhs;
+  a.mask = mask;
+  a.f = f;
+  a.red = red;
+  dim3 grid = grid_for(g, t, nrhs, npar), block(t.bx, t.by, 1);
+  switch (t.nr) {
+    case 4: site_kernel<4><<<grid, block, 0, st>>>(a); break;
+    case 2: site_kernel<2><<<grid, block, 0, st>>>(a); break;
+    default: site_kernel<1><<<grid, block, 0, st>>>(a); break;
+  }
+}
+
+// ============================================================== context
+extern "C" int wl_version(void) { return 1; }
+
+extern "C" wl_status wl_ctx_create(const wl_geometry* geom, int device, wl_ctx** out) {
+  if (!geom || !out) WL_FAIL(nullptr, WL_ERR_ARG, "null argument");
+  for (int mu = 0; mu < 4; ++mu)
+    if (geom->dims[mu] < 2 || (geom->dims[mu] & 1))
+      WL_FAIL(nullptr, WL_ERR_ARG, "every lattice extent must be even and >= 2");
+  long long V = (long long)geom->dims[0] * geom->dims[1] * geom->dims[2] * geom->dims[3];
+  if (V > (1LL << 30)) WL_FAIL(nullptr, WL_ERR_ARG, "lattice too large for 32-bit site indices");
+  WL_CUDA(nullptr, cudaSetDevice(device));
+  wl_ctx* c = new wl_ctx();
+  c->device = device;
+  Geom& g = c->g;
+  for (int mu = 0; mu < 4; ++mu) g.L[mu] = geom->dims[mu];
+  g.V = (int)V;
+  g.Vh = (int)(V / 2);
+  g.Lth = g.L[3] / 2;
+  g.strideRow[0] = g.L[1] * g.L[2];
+  g.strideRow[1] = g.L[2];
+  g.strideRow[2] = 1;
+  for (int mu = 0; mu < 4; ++mu) {
+    g.ph_re[mu] = geom->bc_re[mu];
+    g.ph_im[mu] = geom->bc_im[mu];
+    g.ph_on[mu] = (std::fabs(geom->bc_re[mu] - 1.0) > 1e-12 || std::fabs(geom->bc_im[mu]) > 1e-12) ? 1 : 0;
+  }
+  *out = c;
+  return WL_OK;
+}
+
+extern "C" void wl_ctx_destroy(wl_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  wl_release_solve_cache(ctx);
+  if (ctx->tmp) cudaFree(ctx->tmp);
+  delete ctx;
+}
+
+extern "C" const char* wl_last_error(const wl_ctx* ctx) { return ctx ? ctx->err.c_str() : g_static_err.c_str(); }
+
+extern "C" wl_status wl_ctx_set_stream(wl_ctx* ctx, void* stream) {
+  if (!ctx) WL_FAIL(nullptr, WL_ERR_ARG, "null context");
+  ctx->stream = (cudaStream_t)stream;
+  return WL_OK;
+}
+
+extern "C" wl_status wl_ctx_synchronize(wl_ctx* ctx) {
+  if (!ctx) WL_FAIL(nullptr, WL_ERR_ARG, "null context");
+  WL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return WL_OK;
+}
+
+extern "C" wl_status wl_eo_maps(wl_ctx* ctx, int32_t* even, int32_t* odd, int32_t* nbr) {
+  if (!ctx) WL_FAIL(nullptr, WL_ERR_ARG, "null context");
+  const Geom& g = ctx->g;
+  // host restatement of the device index arithmetic (site_from_compact / neighbor)
+  for (int p = 0; p < 2; ++p) {
+    for (int c = 0; c < g.Vh; ++c) {
+      int th = c % g.Lth, row = c / g.Lth;
+      int z = row % g.L[2], r2 = row / g.L[2];
+      int y = r2 % g.L[1], x = r2 / g.L[1];
+      int t = 2 * th + ((p + x + y + z) & 1);
+      int flat = row * g.L[3] + t;
+      if (p == 0 && even) even[c] = flat;
+      if (p == 1 && odd) odd[c] = flat;
+      if (!nbr) continue;
+      int xs[4] = {x, y, z, t};
+      for (int mu = 0; mu < 4; ++mu)
+        for (int dir = 0; dir < 2; ++dir) {
+          int xx[4] = {xs[0], xs[1], xs[2], xs[3]};
+          xx[mu] = (xx[mu] + (dir == 0 ? 1 : -1) + g.L[mu]) % g.L[mu];
+          int f2 = ((xx[0] * g.L[1] + xx[1]) * g.L[2] + xx[2]) * g.L[3] + xx[3];
+          nbr[((long long)(p * 4 + mu) * 2 + dir) * g.Vh + c] = f2 >> 1;
+        }
+    }
+  }
+  return WL_OK;
+}
+
+// ============================================================== gauge
+static wl_status gauge_fill(wl_gauge* G, const void* U) {
+  wl_ctx* ctx = G->ctx;
+  const Geom& g = ctx->g;
+  WL_CUDA(ctx, cudaMemcpyAsync(G->ref_copy, U, (size_t)4 * g.V * 9 * sizeof(double2), cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+  WL_CUDA(ctx, cudaMemsetAsync(G->uerr, 0, sizeof(unsigned int), ctx->stream));
+  GaugeOut o{G->d18, G->d12, G->s12, G->h12, G->uerr};
+  dim3 grid((g.Vh + 127) / 128, 2, 4);
+  gauge_convert_kernel<<<grid, 128, 0, ctx->stream>>>(g, G->ref_copy, o);
+  return check_launch(ctx, "gauge_convert_kernel");
+}
+
+extern "C" wl_status wl_gauge_create(wl_ctx* ctx, const void* U, wl_gauge** out) {
+  if (!ctx || !U || !out) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  const Geom& g = ctx->g;
+  wl_gauge* G = new wl_gauge();
+  G->ctx = ctx;
+  G->id = g_gauge_ids.fetch_add(1);
+  size_t n = (size_t)2 * 4 * g.Vh;
+  cudaError_t e = cudaSuccess;
+  e = e ? e : cudaMalloc(&G->d18, n * 9 * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc(&G->d12, n * 6 * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc(&G->s12, n * 3 * sizeof(float4));
+  if (e == cudaSuccess) e = cudaMalloc(&G->h12, n * 3 * sizeof(uint2));
+  if (e == cudaSuccess) e = cudaMalloc(&G->ref_copy, (size_t)4 * g.V * 9 * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc(&G->uerr, sizeof(unsigned int));
+  if (e != cudaSuccess) {
+    wl_gauge_destroy(G);
+    ctx->err = std::string("gauge allocation: ") + cudaGetErrorString(e);
+    return WL_ERR_OOM;
+  }
+  wl_status st = gauge_fill(G, U);
+  if (st != WL_OK) {
+    wl_gauge_destroy(G);
+    return st;
+  }
+  *out = G;
+  return WL_OK;
+}
+
+extern "C" wl_status wl_gauge_update(wl_gauge* G, const void* U) {
+  if (!G || !U) WL_FAIL(nullptr, WL_ERR_ARG, "null argument");
+  return gauge_fill(G, U);
+}
+
+extern "C" wl_status wl_gauge_unitarity(wl_gauge* G, double* err) {
+  if (!G || !err) WL_FAIL(nullptr, WL_ERR_ARG, "null argument");
+  wl_ctx* ctx = G->ctx;
+  unsigned int bits = 0;
+  WL_CUDA(ctx, cudaMemcpyAsync(&bits, G->uerr, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream));
+  WL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  float f;
+  std::memcpy(&f, &bits, sizeof(f));
+  G->unitarity = f;
+  *err = (double)f;
+  return WL_OK;
+}
+
+extern "C" void wl_gauge_destroy(wl_gauge* G) {
+  if (!G) return;
+  cudaFree(G->d18);
+  cudaFree(G->d12);
+  cudaFree(G->s12);
+  cudaFree(G->h12);
+  cudaFree(G->ref_copy);
+  cudaFree(G->uerr);
+  delete G;
+}
+
+// ============================================================== reference-layout operators
+using RefHopArgs = HopArgs<LinkRefAdapter, SpinorRefAdapter, EpiXpay<SpinorRefAdapter, false>>;
+
+static RefHopArgs ref_args(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const void* self, double a, double b,
+                           int nrhs, int parity0) {
+  RefHopArgs A;
+  std::memset(&A, 0, sizeof(A));
+  const Geom& g = ctx->g;
+  A.g = g;
+  A.links.f.ptr = G->ref_copy;
+  A.links.f.V = g.V;
+  A.src[0].f = sref(in, g);
+  A.src[1].f = A.src[0].f;
+  A.parity0 = parity0;
+  A.nrhs = nrhs;
+  A.mask = nullptr;
+  A.epi.out[0].f = sref(out, g);
+  A.epi.out[1].f = A.epi.out[0].f;
+  A.epi.has_self = self != nullptr;
+  if (self) {
+    A.epi.self[0].f = sref(self, g);
+    A.epi.self[1].f = A.epi.self[0].f;
+  }
+  A.epi.a = nullptr;
+  A.epi.b = nullptr;
+  A.epi.a0 = a;
+  A.epi.b0 = b;
+  return A;
+}
+
+static wl_status ensure_tmp(wl_ctx* ctx, size_t bytes) {
+  if (ctx->tmp_bytes >= bytes) return WL_OK;
+  if (ctx->tmp) {
+    WL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->tmp);
+    ctx->tmp = nullptr;
+    ctx->tmp_bytes = 0;
+  }
+  WL_CUDA(ctx, cudaMalloc(&ctx->tmp, bytes));
+  ctx->tmp_bytes = bytes;
+  return WL_OK;
+}
+
+// out(target parities) = a*self + b*hop(in); npar = 2 for both parities, else target parity0 only
+template <bool DAG>
+static void ref_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const void* self, double a, double b,
+                    int nrhs, int parity0, int npar) {
+  RefHopArgs A = ref_args(ctx, G, in, out, self, a, b, nrhs, parity0);
+  Tune t;
+  t.nr = 1;
+  t.bx = 128;
+  t.by = 1;
+  launch_hop<DAG, IdxFlat>(t, A, npar, ctx->stream);
+}
+
+extern "C" wl_status wl_apply(wl_ctx* ctx, wl_gauge* G, int op, double mass, unsigned flags, const void* in, void* out,
+                              int nrhs) {
+  if (!ctx || !G || !in || !out) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
+  if (in == out) WL_FAIL(ctx, WL_ERR_ARG, "in and out must not alias");
+  if (nrhs <= 0) WL_FAIL(ctx, WL_ERR_ARG, "nrhs must be positive");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  const Geom& g = ctx->g;
+  const double m0 = mass + 4.0;
+  const size_t fbytes = (size_t)nrhs * g.V * 12 * sizeof(double2);
+  const bool norm = (flags & WL_FLAG_NORMALIZED) != 0;
+  cudaStream_t st = ctx->stream;
+  switch (op) {
+    case WL_OP_D: ref_hop<false>(ctx, G, in, out, in, m0, -0.5, nrhs, 0, 2); break;
+    case WL_OP_DDAG: ref_hop<true>(ctx, G, in, out, in, m0, -0.5, nrhs, 0, 2); break;
+    case WL_OP_HOP: ref_hop<false>(ctx, G, in, out, nullptr, 0.0, -0.5, nrhs, 0, 2); break;
+    case WL_OP_HOP_DAG: ref_hop<true>(ctx, G, in, out, nullptr, 0.0, -0.5, nrhs, 0, 2); break;
+    case WL_OP_DDAGD: {
+      wl_status s = ensure_tmp(ctx, fbytes);
+      if (s != WL_OK) return s;
+      ref_hop<false>(ctx, G, in, ctx->tmp, in, m0, -0.5, nrhs, 0, 2);
+      ref_hop<true>(ctx, G, ctx->tmp, out, ctx->tmp, m0, -0.5, nrhs, 0, 2);
+      break;
+    }
+    case WL_OP_K_OE:
+    case WL_OP_K_EO:
+    case WL_OP_KDAG_OE:
+    case WL_OP_KDAG_EO: {
+      const int target = (op == WL_OP_K_OE || op == WL_OP_KDAG_OE) ? 1 : 0;
+      WL_CUDA(ctx, cudaMemsetAsync(out, 0, fbytes, st));
+      if (op == WL_OP_K_OE || op == WL_OP_K_EO) ref_hop<false>(ctx, G, in, out, nullptr, 0.0, -0.5, nrhs, target, 1);
+      else ref_hop<true>(ctx, G, in, out, nullptr, 0.0, -0.5, nrhs, target, 1);
+      break;
+    }
+    case WL_OP_SCHUR_E:
+    case WL_OP_SCHUR_E_DAG:
+    case WL_OP_SCHUR_O: {
+      // t = K_{p'p} x_p (target p' = 1-p); out_p = c0 x_p + c1 * hop(t)
+      const int p = (op == WL_OP_SCHUR_O) ? 1 : 0;
+      const bool dag = (op == WL_OP_SCHUR_E_DAG);
+      wl_status s = ensure_tmp(ctx, fbytes);
+      if (s != WL_OK) return s;
+      WL_CUDA(ctx, cudaMemsetAsync(out, 0, fbytes, st));
+      const double c0 = norm ? 1.0 : m0;
+      const double c1 = norm ? 0.5 / (m0 * m0) : 0.5 / m0;
+      if (dag) {
+        ref_hop<true>(ctx, G, in, ctx->tmp, nullptr, 0.0, -0.5, nrhs, 1 - p, 1);
+        ref_hop<true>(ctx, G, ctx->tmp, out, in, c0, c1, nrhs, p, 1);
+      } else {
+        ref_hop<false>(ctx, G, in, ctx->tmp, nullptr, 0.0, -0.5, nrhs, 1 - p, 1);
+        ref_hop<false>(ctx, G, ctx->tmp, out, in, c0, c1, nrhs, p, 1);
+      }
+      break;
+    }
+    case WL_OP_SCHUR_E_NORMAL: {
+      // out = S^dag S x (normalized or not), via two Schur applications
+      wl_status s = ensure_tmp(ctx, 2 * fbytes);
+      if (s != WL_OK) return s;
+      void* t1 = ctx->tmp;
+      void* y = (char*)ctx->tmp + fbytes;
+      WL_CUDA(ctx, cudaMemsetAsync(y, 0, fbytes, st));
+      WL_CUDA(ctx, cudaMemsetAsync(out, 0, fbytes, st));
+      const double c0 = norm ? 1.0 : m0;
+      const double c1 = norm ? 0.5 / (m0 * m0) : 0.5 / m0;
+      ref_hop<false>(ctx, G, in, t1, nullptr, 0.0, -0.5, nrhs, 1, 1);
+      ref_hop<false>(ctx, G, t1, y, in, c0, c1, nrhs, 0, 1);
+      ref_hop<true>(ctx, G, y, t1, nullptr, 0.0, -0.5, nrhs, 1, 1);
+      ref_hop<true>(ctx, G, t1, out, y, c0, c1, nrhs, 0, 1);
+      break;
+    }
+    default: WL_FAIL(ctx, WL_ERR_ARG, "unknown operator");
+  }
+  return check_launch(ctx, "wl_apply");
+}
+
+// ============================================================== force
+extern "C" wl_status wl_pf_force(wl_ctx* ctx, wl_gauge* G, const void* X, const void* Y, double coef, int accumulate,
+                                 void* F) {
+  if (!ctx || !G || !X || !Y || !F) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  const Geom& g = ctx->g;
+  ForceArgs A;
+  A.g = g;
+  A.U.ptr = G->ref_copy;
+  A.U.V = g.V;
+  A.X = sref(X, g);
+  A.Y = sref(Y, g);
+  A.F = (double2*)F;
+  A.coef = coef;
+  A.accumulate = accumulate;
+  dim3 grid((g.Vh + 127) / 128, 2, 4);
+  pf_force_kernel<<<grid, 128, 0, ctx->stream>>>(A);
+  return check_launch(ctx, "pf_force_kernel");
+}
+
+// ============================================================== CG engine
+namespace {
+
+struct TuneKey {
+  int vh, prec, nslots, op;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(vh, prec, nslots, op) < std::tie(o.vh, o.prec, o.nslots, o.op);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, Tune> g_tune_cache;
+
+}  // namespace
+
+struct wl_engine {
+  wl_ctx* ctx = nullptr;
+  wl_gauge* gauge = nullptr;
+  unsigned long long gauge_id = 0;  // id of the gauge the graph was captured with
+  wl_solve_params prm;
+  int n = 0;        // slots
+  int npar = 1;     // 1 for EO (even fields), 2 for full lattice
+  int sprec = 0;
+  Tune ts, td, tsite;  // sloppy hop, FP64 hop, site kernels
+  // fields
+  IField b64, x64, y64, t64;  // FP64
+  IField xs, rs, p, y, t1;    // sloppy (t1 reused for t2)
+  // scalars (device)
+  double* dbl = nullptr;
+  int* ints = nullptr;
+  double *r2, *r2_new, *pAp, *r2_true, *rmax2, *b2, *tol2, *beta, *one, *neg_half, *half_alpha, *m0;
+  int *active, *ru, *iters, *maxiter, *status, *n_ru, *n_active, *admit;
+  // host mirrors of parameters
+  std::vector<double> h_tol2, h_one, h_neg_half, h_half_alpha, h_m0;
+  std::vector<int> h_maxiter, h_admit;
+  int* h_pinned = nullptr;
+  // reductions
+  double* partials = nullptr;
+  unsigned* counters = nullptr;
+  // graph
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_built = false;
+};
+
+static const int kEngineDoubles = 12;
+static const int kEngineInts = 8;
+
+int64_t engine_bytes_impl(const Geom& g, int op, int sprec, int n) {
+  const int npar = (op == WL_SOLVE_EO_NORMAL) ? 1 : 2;
+  int64_t b = 0;
+  b += 3 * (int64_t)field_bytes(P_DOUBLE, g.Vh, n, npar);                // b64, x64, y64
+  b += (int64_t)field_bytes(P_DOUBLE, g.Vh, n, op == WL_SOLVE_EO_NORMAL ? 1 : 2);  // t64
+  b += 4 * (int64_t)field_bytes(sprec, g.Vh, n, npar);                   // xs, rs, p, y
+  b += (int64_t)field_bytes(sprec, g.Vh, n, 1);                          // t1
+  b += (int64_t)n * (g.Vh / 32 + 1) * 2 * sizeof(double) + 4096;
+  return b;
+}
+
+extern "C" int64_t wl_engine_bytes(const wl_ctx* ctx, int op, int inner_prec, int nslots) {
+  if (!ctx) return -1;
+  return engine_bytes_impl(ctx->g, op, inner_prec, nslots);
+}
+
+static Reduce red_to(wl_engine* E, double* result) {
+  Reduce r;
+  r.partials = E->partials;
+  r.counter = E->counters;
+  r.result = result;
+  return r;
+}
+
+__global__ void admit_state_kernel(CGScalars S, const int* admit, int use_x0, int n) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  int local = 0;
+  for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    if (admit[s]) {
+      S.iters[s] = 0;
+      S.n_ru[s] = 0;
+      const double r2 = use_x0 ? S.r2_true[s] : S.b2[s];
+      S.r2[s] = r2;
+      S.rmax2[s] = r2;
+      S.beta[s] = 0.0;
+      if (!(S.b2[s] > 0.0) || r2 <= S.tol2[s] * S.b2[s]) {
+        S.active[s] = 0;
+        S.status[s] = ST_CONVERGED;
+      } else if (!isfinite(r2)) {
+        S.active[s] = 0;
+        S.status[s] = ST_NAN;
+      } else {
+        S.active[s] = 1;
+        S.status[s] = ST_RUNNING;
+      }
+    }
+    local += S.active[s];
+  }
+  atomicAdd(&cnt, local);
+  __syncthreads();
+  if (threadIdx.x == 0) *S.n_active = cnt;
+}
+
+// Maps admitted slot -> index in the caller's b buffer
+struct FPackMapped {
+  static constexpr bool kReduce = true;
+  Geom g;
+  SpinorRef in;
+  const int* map;
+  SpinorField<P_DOUBLE> out[2];
+  WL_D double operator()(int rhs, int parity, int c) const {
+    const long long f = flat_of(g, parity, c);
+    Spinor<double> s;
+    in.load(s, map[rhs], f);
+    out[parity].store(s, rhs, c);
+    return snorm2(s);
+  }
+};
+
+static CGScalars scalars_of(wl_engine* E) {
+  CGScalars S;
+  S.r2 = E->r2;
+  S.r2_new = E->r2_new;
+  S.pAp = E->pAp;
+  S.r2_true = E->r2_true;
+  S.rmax2 = E->rmax2;
+  S.b2 = E->b2;
+  S.tol2 = E->tol2;
+  S.beta = E->beta;
+  S.active = E->active;
+  S.ru = E->ru;
+  S.iters = E->iters;
+  S.maxiter = E->maxiter;
+  S.status = E->status;
+  S.n_ru = E->n_ru;
+  S.n_active = E->n_active;
+  S.delta2 = E->prm.delta * E->prm.delta;
+  return S;
+}
+
+template <int S> struct SloppyLinks;
+template <> struct SloppyLinks<P_DOUBLE> {
+  using type = LinkField<L_D18>;
+  static type get(wl_gauge* G) { return type{G->d18, G->ctx->g.Vh}; }
+};
+template <> struct SloppyLinks<P_SINGLE> {
+  using type = LinkField<L_S12>;
+  static type get(wl_gauge* G) { return type{G->s12, G->ctx->g.Vh}; }
+};
+template <> struct SloppyLinks<P_HALF> {
+  using type = LinkField<L_H12>;
+  static type get(wl_gauge* G) { return type{G->h12, G->ctx->g.Vh}; }
+};
+
+// Enqueue the FP64 normal operator on x64 ending in the true residual
+// rs = convert(b - A x64), r2_true = |b - A x64|^2, for the slots in `mask`.
+template <int S>
+static void enqueue_true_residual(wl_engine* E, const int* mask, cudaStream_t st) {
+  using SFS = SpinorField<S>;
+  using SFD = SpinorField<P_DOUBLE>;
+  const Geom& g = E->ctx->g;
+  LinkField<L_D18> LD{E->gauge->d18, g.Vh};
+  const bool eo = E->prm.op == WL_SOLVE_EO_NORMAL;
+  if (eo) {
+    {  // t64 = K_oe x64
+      HopArgs<LinkField<L_D18>, SFD, EpiXpay<SFD, false>> A{};
+      A.g = g; A.links = LD; sf2<P_DOUBLE>(E->x64, A.src); A.parity0 = 1; A.nrhs = E->n; A.mask = mask;
+      sf2<P_DOUBLE>(E->t64, A.epi.out); A.epi.has_self = 0; A.epi.b = E->neg_half;
+      launch_hop<false, IdxCompact>(E->td, A, 1, st);
+    }
+    {  // y64 = x64 + (alpha/2) hop(t64)
+      HopArgs<LinkField<L_D18>, SFD, EpiXpay<SFD, false>> A{};
+      A.g = g; A.links = LD; sf2<P_DOUBLE>(E->t64, A.src); A.parity0 = 0; A.nrhs = E->n; A.mask = mask;
+      sf2<P_DOUBLE>(E->y64, A.epi.out); sf2<P_DOUBLE>(E->x64, A.epi.self); A.epi.has_self = 1;
+      A.epi.a = E->one; A.epi.b = E->half_alpha;
+      launch_hop<false, IdxCompact>(E->td, A, 1, st);
+    }
+    {  // t64 = Kdag_oe y64
+      HopArgs<LinkField<L_D18>, SFD, EpiXpay<SFD, false>> A{};
+      A.g = g; A.links = LD; sf2<P_DOUBLE>(E->y64, A.src); A.parity0 = 1; A.nrhs = E->n; A.mask = mask;
+      sf2<P_DOUBLE>(E->t64, A.epi.out); A.epi.has_self = 0; A.epi.b = E->neg_half;
+      launch_hop<true, IdxCompact>(E->td, A, 1, st);
+    }
+    {  // rs = b - (y64 + (alpha/2) hopdag(t64))
+      HopArgs<LinkField<L_D18>, SFD, EpiResid<SFS>> A{};
+      A.g = g; A.links = LD; sf2<P_DOUBLE>(E->t64, A.src); A.parity0 = 0; A.nrhs = E->n; A.mask = mask;
+      sf2<P_DOUBLE>(E->y64, A.epi.y); sf2<P_DOUBLE>(E->b64, A.epi.bvec); sf2<S>(E->rs, A.epi.rs);
+      A.epi.a = E->one; A.epi.b = E->half_alpha;
+      A.red = red_to(E, E->r2_true);
+      launch_hop<true, IdxCompact>(E->td, A, 1, st);
+    }
+  } else {
+    {  // y64 = D x64
+      HopArgs<LinkField<L_D18>, SFD, EpiXpay<SFD, false>> A{};
+      A.g = g; A.links = LD; sf2<P_DOUBLE>(E->x64, A.src); A.parity0 = 0; A.nrhs = E->n; A.mask = mask;
+      sf2<P_DOUBLE>(E->y64, A.epi.out); sf2<P_DOUBLE>(E->x64, A.epi.self); A.epi.has_self = 1;
+      A.epi.a = E->m0; A.epi.b = E->neg_half;
+      launch_hop<false, IdxCompact>(E->td, A, 2, st);
+    }
+    {  // rs = b - D^dag y64
+      HopArgs<LinkField<L_D18>, SFD, EpiResid<SFS>> A{};
+      A.g = g; A.links = LD; sf2<P_DOUBLE>(E->y64, A.src); A.parity0 = 0; A.nrhs = E->n; A.mask = mask;
+      sf2<P_DOUBLE>(E->y64, A.epi.y); sf2<P_DOUBLE>(E->b64, A.epi.bvec); sf2<S>(E->rs, A.epi.rs);
+      A.epi.a = E->m0; A.epi.b = E->neg_half;
+      A.red = red_to(E, E->r2_true);
+      launch_hop<true, IdxCompact>(E->td, A, 2, st);
+    }
+  }
+}
+
+// One CG iteration for all active slots.
+template <int S>
+static void enqueue_iteration(wl_engine* E, cudaStream_t st) {
+  using SFS = SpinorField<S>;
+  using LS = typename SloppyLinks<S>::type;
+  const Geom& g = E->ctx->g;
+  LS L = SloppyLinks<S>::get(E->gauge);
+  const bool eo = E->prm.op == WL_SOLVE_EO_NORMAL;
+  const int n = E->n;
+  if (eo) {
+    {  // t1 = K_oe p
+      HopArgs<LS, SFS, EpiXpay<SFS, false>> A{};
+      A.g = g; A.links = L; sf2<S>(E->p, A.src); A.parity0 = 1; A.nrhs = n; A.mask = E->active;
+      sf2<S>(E->t1, A.epi.out); A.epi.has_self = 0; A.epi.b = E->neg_half;
+      launch_hop<false, IdxCompact>(E->ts, A, 1, st);
+    }
+    {  // y = p + (alpha/2) hop(t1) = M p ; pAp = |y|^2
+      HopArgs<LS, SFS, EpiXpay<SFS, true>> A{};
+      A.g = g; A.links = L; sf2<S>(E->t1, A.src); A.parity0 = 0; A.nrhs = n; A.mask = E->active;
+      sf2<S>(E->y, A.epi.out); sf2<S>(E->p, A.epi.self); A.epi.has_self = 1;
+      A.epi.a = E->one; A.epi.b = E->half_alpha;
+      A.red = red_to(E, E->pAp);
+      launch_hop<false, IdxCompact>(E->ts, A, 1, st);
+    }
+    {  // t2 = Kdag_oe y
+      HopArgs<LS, SFS, EpiXpay<SFS, false>> A{};
+      A.g = g; A.links = L; sf2<S>(E->y, A.src); A.parity0 = 1; A.nrhs = n; A.mask = E->active;
+      sf2<S>(E->t1, A.epi.out); A.epi.has_self = 0; A.epi.b = E->neg_half;
+      launch_hop<true, IdxCompact>(E->ts, A, 1, st);
+    }
+    {  // Ap = M^dag y ; CG update
+      HopArgs<LS, SFS, EpiCG<SFS>> A{};
+      A.g = g; A.links = L; sf2<S>(E->t1, A.src); A.parity0 = 0; A.nrhs = n; A.mask = E->active;
+      sf2<S>(E->y, A.epi.y); sf2<S>(E->p, A.epi.p); sf2<S>(E->xs, A.epi.xs); sf2<S>(E->rs, A.epi.rs);
+      A.epi.a = E->one; A.epi.b = E->half_alpha; A.epi.r2 = E->r2; A.epi.pAp = E->pAp;
+      A.red = red_to(E, E->r2_new);
+      launch_hop<true, IdxCompact>(E->ts, A, 1, st);
+    }
+  } else {
+    {  // y = D p ; pAp = |y|^2
+      HopArgs<LS, SFS, EpiXpay<SFS, true>> A{};
+      A.g = g; A.links = L; sf2<S>(E->p, A.src); A.parity0 = 0; A.nrhs = n; A.mask = E->active;
+      sf2<S>(E->y, A.epi.out); sf2<S>(E->p, A.epi.self); A.epi.has_self = 1;
+      A.epi.a = E->m0; A.epi.b = E->neg_half;
+      A.red = red_to(E, E->pAp);
+      launch_hop<false, IdxCompact>(E->ts, A, 2, st);
+    }
+    {  // Ap = D^dag y ; CG update
+      HopArgs<LS, SFS, EpiCG<SFS>> A{};
+      A.g = g; A.links = L; sf2<S>(E->y, A.src); A.parity0 = 0; A.nrhs = n; A.mask = E->active;
+      sf2<S>(E->y, A.epi.y); sf2<S>(E->p, A.epi.p); sf2<S>(E->xs, A.epi.xs); sf2<S>(E->rs, A.epi.rs);
+      A.epi.a = E->m0; A.epi.b = E->neg_half; A.epi.r2 = E->r2; A.epi.pAp = E->pAp;
+      A.red = red_to(E, E->r2_new);
+      launch_hop<true, IdxCompact>(E->ts, A, 2, st);
+    }
+  }
+  CGScalars Sc = scalars_of(E);
+  cg_decide_kernel<<<1, 128, 0, st>>>(Sc, n);
+  {  // x64 += xs ; xs = 0  (reliable-update slots)
+    FAccumX<SFS> f;
+    sf2<P_DOUBLE>(E->x64, f.x);
+    sf2<S>(E->xs, f.xs);
+    launch_site(E->tsite, g, 0, E->npar, n, E->ru, f, Reduce{}, st);
+  }
+  enqueue_true_residual<S>(E, E->ru, st);
+  cg_finalize_kernel<<<1, 128, 0, st>>>(Sc, n);
+  {  // p = rs + beta p
+    FUpdateP<SFS> f;
+    sf2<S>(E->rs, f.rs);
+    sf2<S>(E->p, f.p);
+    f.beta = E->beta;
+    launch_site(E->tsite, g, 0, E->npar, n, E->active, f, Reduce{}, st);
+  }
+}
+
+template <int S>
+static void enqueue_admit(wl_engine* E, const void* b, int use_x0, const void* x0, const int* map_dev,
+                          cudaStream_t st) {
+  using SFS = SpinorField<S>;
+  using SFD = SpinorField<P_DOUBLE>;
+  const Geom& g = E->ctx->g;
+  const int n = E->n;
+  const int* adm = E->admit;
+  const int par0 = 0;
+  {  // b64 <- b ; b2
+    FPackMapped f;
+    f.g = g;
+    f.in = sref(b, g);
+    f.map = map_dev;
+    sf2<P_DOUBLE>(E->b64, f.out);
+    launch_site(E->tsite, g, par0, E->npar, n, adm, f, red_to(E, E->b2), st);
+  }
+  if (use_x0) {
+    FPackMapped f;
+    f.g = g;
+    f.in = sref(x0, g);
+    f.map = map_dev;
+    sf2<P_DOUBLE>(E->x64, f.out);
+    launch_site(E->tsite, g, par0, E->npar, n, adm, f, red_to(E, E->r2_true), st);
+    enqueue_true_residual<S>(E, adm, st);
+  } else {
+    FZero<SFD> z;
+    sf2<P_DOUBLE>(E->x64, z.out);
+    launch_site(E->tsite, g, par0, E->npar, n, adm, z, Reduce{}, st);
+    FConvert<SFD, SFS> cv;
+    sf2<P_DOUBLE>(E->b64, cv.in);
+    sf2<S>(E->rs, cv.out);
+    launch_site(E->tsite, g, par0, E->npar, n, adm, cv, red_to(E, E->r2_true), st);
+  }
+  {  // p = rs ; xs = 0
+    FConvert<SFS, SFS> cv;
+    sf2<S>(E->rs, cv.in);
+    sf2<S>(E->p, cv.out);
+    launch_site(E->tsite, g, par0, E->npar, n, adm, cv, red_to(E, E->pAp), st);
+    FZero<SFS> z;
+    sf2<S>(E->xs, z.out);
+    launch_site(E->tsite, g, par0, E->npar, n, adm, z, Reduce{}, st);
+  }
+  admit_state_kernel<<<1, 128, 0, st>>>(scalars_of(E), adm, use_x0, n);
+}
+
+static void enqueue_iteration_any(wl_engine* E, cudaStream_t st) {
+  switch (E->sprec) {
+    case P_HALF: enqueue_iteration<P_HALF>(E, st); break;
+    case P_SINGLE: enqueue_iteration<P_SINGLE>(E, st); break;
+    default: enqueue_iteration<P_DOUBLE>(E, st); break;
+  }
+}
+
+// ------------------------------------------------------------------ autotune
+// Times the sloppy hop kernel (the dominant cost) over candidate
+// (RHS per thread, sites per block, RHS groups per block) shapes and keeps
+// the fastest for this (volume, precision, slot count, operator).
+template <int S>
+static Tune autotune_hop(wl_engine* E, cudaStream_t st) {
+  using SFS = SpinorField<S>;
+  using LS = typename SloppyLinks<S>::type;
+  const Geom& g = E->ctx->g;
+  const int n = E->n;
+  std::vector<Tune> cands;
+  for (int nr : {1, 2, 4}) {
+    if (nr > 1 && nr > n) continue;
+    int groups = (n + nr - 1) / nr;
+    for (int bx : {64, 128, 256})
+      for (int by : {1, 2, 4, 8}) {
+        if (bx * by > 256 || by * nr > kMaxRB || (by > 1 && by > groups)) continue;
+        cands.push_back(Tune{nr, bx, by});
+      }
+  }
+  Tune best = cands.front();
+  float best_ms = 1e30f;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  HopArgs<LS, SFS, EpiXpay<SFS, false>> A{};
+  A.g = g;
+  A.links = SloppyLinks<S>::get(E->gauge);
+  sf2<S>(E->p, A.src);
+  A.parity0 = 1;
+  A.nrhs = n;
+  A.mask = nullptr;
+  sf2<S>(E->t1, A.epi.out);
+  A.epi.has_self = 0;
+  A.epi.b = E->neg_half;
+  const int reps = g.Vh >= 65536 ? 5 : 20;
+  for (const Tune& t : cands) {
+    launch_hop<false, IdxCompact>(t, A, 1, st);
+    cudaEventRecord(e0, st);
+    for (int i = 0; i < reps; ++i) launch_hop<false, IdxCompact>(t, A, 1, st);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (cudaGetLastError() == cudaSuccess && ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
+}
+
+static Tune pick_tune(wl_engine* E, cudaStream_t st) {
+  TuneKey k{E->ctx->g.Vh, E->sprec, E->n, E->prm.op};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(k);
+    if (it != g_tune_cache.end()) return it->second;
+  }
+  Tune t;
+  const char* env = std::getenv("WL_AUTOTUNE");
+  const bool on = !(env && env[0] == '0');
+  if (on) {
+    switch (E->sprec) {
+      case P_HALF: t = autotune_hop<P_HALF>(E, st); break;
+      case P_SINGLE: t = autotune_hop<P_SINGLE>(E, st); break;
+      default: t = autotune_hop<P_DOUBLE>(E, st); break;
+    }
+  } else {
+    t.nr = E->n >= 2 ? 2 : 1;
+    t.bx = 128;
+    t.by = std::max(1, std::min(4, (E->n + t.nr - 1) / t.nr));
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[k] = t;
+  return t;
+}
+
+// ------------------------------------------------------------------ engine API
+struct EngineStream {
+  cudaStream_t st;
+};
+static std::map<const wl_engine*, cudaStream_t> g_engine_streams;
+static std::mutex g_es_mu;
+
+static cudaStream_t engine_stream(const wl_engine* E) {
+  std::lock_guard<std::mutex> lk(g_es_mu);
+  return g_engine_streams[E];
+}
+
+extern "C" void wl_engine_destroy(wl_engine* E) {
+  if (!E) return;
+  cudaSetDevice(E->ctx->device);
+  cudaStream_t st = engine_stream(E);
+  if (st) cudaStreamSynchronize(st);
+  if (E->gexec) cudaGraphExecDestroy(E->gexec);
+  IField* fs[] = {&E->b64, &E->x64, &E->y64, &E->t64, &E->xs, &E->rs, &E->p, &E->y, &E->t1};
+  for (IField* f : fs) free_field(*f);
+  cudaFree(E->dbl);
+  cudaFree(E->ints);
+  cudaFree(E->partials);
+  cudaFree(E->counters);
+  if (E->h_pinned) cudaFreeHost(E->h_pinned);
+  if (st) cudaStreamDestroy(st);
+  {
+    std::lock_guard<std::mutex> lk(g_es_mu);
+    g_engine_streams.erase(E);
+  }
+  delete E;
+}
+
+extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_params* prm, int nslots,
+                                      wl_engine** out) {
+  if (!ctx || !G || !prm || !out) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
+  if (nslots <= 0 || nslots > 4096) WL_FAIL(ctx, WL_ERR_ARG, "nslots out of range");
+  if (prm->op != WL_SOLVE_NORMAL && prm->op != WL_SOLVE_EO_NORMAL) WL_FAIL(ctx, WL_ERR_ARG, "unknown solve op");
+  if (prm->inner_prec < 0 || prm->inner_prec > 2) WL_FAIL(ctx, WL_ERR_ARG, "unknown inner precision");
+  if (!(prm->tol > 0.0)) WL_FAIL(ctx, WL_ERR_ARG, "tol must be positive");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  wl_engine* E = new wl_engine();
+  E->ctx = ctx;
+  E->gauge = G;
+  E->prm = *prm;
+  if (E->prm.maxiter <= 0) E->prm.maxiter = 1000;
+  if (E->prm.check_every <= 0) E->prm.check_every = 8;
+  E->n = nslots;
+  E->npar = prm->op == WL_SOLVE_EO_NORMAL ? 1 : 2;
+  E->sprec = prm->inner_prec;
+  // 12-real reconstruction is exact only for SU(3) links: fall back to FP64
+  // 18-real iteration when the uploaded links are not unitary.
+  double uerr = 0.0;
+  wl_status s0 = wl_gauge_unitarity(G, &uerr);
+  if (s0 != WL_OK) {
+    delete E;
+    return s0;
+  }
+  if (E->sprec != P_DOUBLE && !(uerr < 1e-4)) E->sprec = P_DOUBLE;
+  cudaStream_t st;
+  WL_CUDA(ctx, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  {
+    std::lock_guard<std::mutex> lk(g_es_mu);
+    g_engine_streams[E] = st;
+  }
+  const Geom& g = ctx->g;
+  const int n = nslots;
+  wl_status s = WL_OK;
+  cudaStream_t keep = ctx->stream;
+  ctx->stream = st;
+  const int tpar = prm->op == WL_SOLVE_EO_NORMAL ? 1 : 2;
+  if (s == WL_OK) s = alloc_field(ctx, E->b64, P_DOUBLE, g.Vh, n, E->npar);
+  if (s == WL_OK) s = alloc_field(ctx, E->x64, P_DOUBLE, g.Vh, n, E->npar);
+  if (s == WL_OK) s = alloc_field(ctx, E->y64, P_DOUBLE, g.Vh, n, E->npar);
+  if (s == WL_OK) s = alloc_field(ctx, E->t64, P_DOUBLE, g.Vh, n, tpar);
+  if (s == WL_OK) s = alloc_field(ctx, E->xs, E->sprec, g.Vh, n, E->npar);
+  if (s == WL_OK) s = alloc_field(ctx, E->rs, E->sprec, g.Vh, n, E->npar);
+  if (s == WL_OK) s = alloc_field(ctx, E->p, E->sprec, g.Vh, n, E->npar);
+  if (s == WL_OK) s = alloc_field(ctx, E->y, E->sprec, g.Vh, n, E->npar);
+  if (s == WL_OK) s = alloc_field(ctx, E->t1, E->sprec, g.Vh, n, 1);
+  ctx->stream = keep;
+  if (s != WL_OK) {
+    wl_engine_destroy(E);
+    return s;
+  }
+  cudaError_t e = cudaMalloc(&E->dbl, sizeof(double) * kEngineDoubles * n);
+  if (e == cudaSuccess) e = cudaMalloc(&E->ints, sizeof(int) * (kEngineInts * n + 1));
+  const size_t nblk = (size_t)((g.Vh + 31) / 32) * 2;
+  if (e == cudaSuccess) e = cudaMalloc(&E->partials, sizeof(double) * nblk * n);
+  if (e == cudaSuccess) e = cudaMalloc(&E->counters, sizeof(unsigned) * (n + 1));
+  if (e == cudaSuccess) e = cudaMallocHost(&E->h_pinned, sizeof(int) * (3 * n + 1));
+  if (e != cudaSuccess) {
+    ctx->err = std::string("engine allocation: ") + cudaGetErrorString(e);
+    wl_engine_destroy(E);
+    return WL_ERR_OOM;
+  }
+  cudaMemsetAsync(E->dbl, 0, sizeof(double) * kEngineDoubles * n, st);
+  cudaMemsetAsync(E->ints, 0, sizeof(int) * (kEngineInts * n + 1), st);
+  cudaMemsetAsync(E->counters, 0, sizeof(unsigned) * (n + 1), st);
+  double* d = E->dbl;
+  E->r2 = d + 0 * n; E->r2_new = d + 1 * n; E->pAp = d + 2 * n; E->r2_true = d + 3 * n;
+  E->rmax2 = d + 4 * n; E->b2 = d + 5 * n; E->tol2 = d + 6 * n; E->beta = d + 7 * n;
+  E->one = d + 8 * n; E->neg_half = d + 9 * n; E->half_alpha = d + 10 * n; E->m0 = d + 11 * n;
+  int* I = E->ints;
+  E->active = I + 0 * n; E->ru = I + 1 * n; E->iters = I + 2 * n; E->maxiter = I + 3 * n;
+  E->status = I + 4 * n; E->n_ru = I + 5 * n; E->admit = I + 6 * n; E->n_active = I + 8 * n;
+  // I + 7n .. 8n: slot -> caller index map
+  E->h_tol2.assign(n, 0.0);
+  E->h_one.assign(n, 1.0);
+  E->h_neg_half.assign(n, -0.5);
+  E->h_half_alpha.assign(n, 0.0);
+  E->h_m0.assign(n, 4.0);
+  E->h_maxiter.assign(n, E->prm.maxiter);
+  E->ts = pick_tune(E, st);
+  E->td = Tune{1, 128, 1};
+  E->tsite = Tune{1, 128, 1};
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("engine set-up: ") + cudaGetErrorString(e);
+    wl_engine_destroy(E);
+    return WL_ERR_CUDA;
+  }
+  *out = E;
+  return WL_OK;
+}
+
+static wl_status admit_impl(wl_engine* E, const int* slots, int nadm, const void* b, const void* x0,
+                            const double* masses, const double* tols, const int* maxiters) {
+  if (!E || !slots || !b || !masses) WL_FAIL(nullptr, WL_ERR_ARG, "null argument");
+  wl_ctx* ctx = E->ctx;
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int n = E->n;
+  std::vector<int> adm(n, 0), map(n, 0);
+  for (int i = 0; i < nadm; ++i) {
+    int s = slots[i];
+    if (s < 0 || s >= n) WL_FAIL(ctx, WL_ERR_ARG, "slot index out of range");
+    adm[s] = 1;
+    map[s] = i;
+    const double m0 = masses[i] + 4.0;
+    if (!(std::fabs(m0) > 1e-12)) WL_FAIL(ctx, WL_ERR_ARG, "m0 = mass + 4 must be non-zero");
+    const double tol = tols ? tols[i] : E->prm.tol;
+    E->h_tol2[s] = tol * tol;
+    E->h_m0[s] = m0;
+    E->h_half_alpha[s] = 0.5 / (m0 * m0);
+    E->h_maxiter[s] = maxiters ? maxiters[i] : E->prm.maxiter;
+  }
+  cudaStream_t st = engine_stream(E);
+  // order after work already queued on the caller's stream (b may have been produced there)
+  cudaEvent_t ev;
+  WL_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaEventRecord(ev, ctx->stream);
+  cudaStreamWaitEvent(st, ev, 0);
+  cudaEventDestroy(ev);
+  WL_CUDA(ctx, cudaMemcpyAsync(E->admit, adm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->ints + 7 * n, map.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->tol2, E->h_tol2.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->one, E->h_one.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->neg_half, E->h_neg_half.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->half_alpha, E->h_half_alpha.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->m0, E->h_m0.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->maxiter, E->h_maxiter.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  // host vectors must outlive the async copies
+  WL_CUDA(ctx, cudaStreamSynchronize(st));
+  const int use_x0 = x0 != nullptr;
+  switch (E->sprec) {
+    case P_HALF: enqueue_admit<P_HALF>(E, b, use_x0, x0, E->ints + 7 * n, st); break;
+    case P_SINGLE: enqueue_admit<P_SINGLE>(E, b, use_x0, x0, E->ints + 7 * n, st); break;
+    default: enqueue_admit<P_DOUBLE>(E, b, use_x0, x0, E->ints + 7 * n, st); break;
+  }
+  return check_launch(ctx, "wl_engine_admit");
+}
+
+extern "C" wl_status wl_engine_admit(wl_engine* E, const int* slots, int nadm, const void* b, const double* masses,
+                                     const double* tols, const int* maxiters) {
+  return admit_impl(E, slots, nadm, b, nullptr, masses, tols, maxiters);
+}
+
+static wl_status engine_admit_all(wl_engine* E, const void* b, const void* x0, const double* masses) {
+  const int n = E->n;
+  std::vector<int> slots(n);
+  for (int i = 0; i < n; ++i) slots[i] = i;
+  return admit_impl(E, slots.data(), n, b, x0, masses, nullptr, nullptr);
+}
+
+static wl_status build_graph(wl_engine* E, cudaStream_t st) {
+  wl_ctx* ctx = E->ctx;
+  cudaGraph_t graph;
+  WL_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  enqueue_iteration_any(E, st);
+  cudaError_t e = cudaStreamEndCapture(st, &graph);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("graph capture: ") + cudaGetErrorString(e);
+    return WL_ERR_CUDA;
+  }
+  e = cudaGraphInstantiate(&E->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("graph instantiate: ") + cudaGetErrorString(e);
+    E->gexec = nullptr;
+    return WL_ERR_CUDA;
+  }
+  E->graph_built = true;
+  return WL_OK;
+}
+
+extern "C" wl_status wl_engine_step(wl_engine* E, int iters) {
+  if (!E) WL_FAIL(nullptr, WL_ERR_ARG, "null engine");
+  wl_ctx* ctx = E->ctx;
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = engine_stream(E);
+  if (E->prm.use_graph && E->graph_built && E->gauge_id != E->gauge->id) {
+    cudaGraphExecDestroy(E->gexec);
+    E->gexec = nullptr;
+    E->graph_built = false;
+  }
+  if (E->prm.use_graph && !E->graph_built) {
+    E->gauge_id = E->gauge->id;
+    wl_status s = build_graph(E, st);
+    if (s != WL_OK) return s;
+  }
+  for (int i = 0; i < iters; ++i) {
+    if (E->prm.use_graph) WL_CUDA(ctx, cudaGraphLaunch(E->gexec, st));
+    else enqueue_iteration_any(E, st);
+  }
+  return check_launch(ctx, "wl_engine_step");
+}
+
+extern "C" wl_status wl_engine_poll(wl_engine* E, int* status, int* n_active) {
+  if (!E) WL_FAIL(nullptr, WL_ERR_ARG, "null engine");
+  wl_ctx* ctx = E->ctx;
+  cudaStream_t st = engine_stream(E);
+  const int n = E->n;
+  WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned, E->n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (status) WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned + 1, E->status, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  WL_CUDA(ctx, cudaStreamSynchronize(st));
+  if (n_active) *n_active = E->h_pinned[0];
+  if (status) std::memcpy(status, E->h_pinned + 1, sizeof(int) * n);
+  return WL_OK;
+}
+
+static wl_status engine_stats(wl_engine* E, wl_solve_stats* stats, int first, int count) {
+  wl_ctx* ctx = E->ctx;
+  cudaStream_t st = engine_stream(E);
+  const int n = E->n;
+  std::vector<int> it(n), sts(n), nru(n);
+  std::vector<double> r2(n), b2(n);
+  WL_CUDA(ctx, cudaMemcpyAsync(it.data(), E->iters, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(sts.data(), E->status, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(nru.data(), E->n_ru, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(r2.data(), E->r2, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(b2.data(), E->b2, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  WL_CUDA(ctx, cudaStreamSynchronize(st));
+  for (int i = 0; i < count; ++i) {
+    const int s = first + i;
+    stats[i].iters = it[s];
+    stats[i].reliable_updates = nru[s];
+    stats[i].status = sts[s];
+    stats[i].true_res = b2[s] > 0.0 ? std::sqrt(std::max(r2[s], 0.0) / b2[s]) : 0.0;
+  }
+  return WL_OK;
+}
+
+static wl_status engine_unpack(wl_engine* E, int first, int count, void* x) {
+  wl_ctx* ctx = E->ctx;
+  cudaStream_t st = engine_stream(E);
+  const Geom& g = ctx->g;
+  IField view = E->x64;
+  view.data = (char*)E->x64.data + (size_t)first * view.rstride() * 16;
+  view.nrhs = count;
+  FUnpack f;
+  f.g = g;
+  sf2<P_DOUBLE>(view, f.in);
+  f.out = sref(x, g);
+  f.rhs_off = 0;
+  launch_site(E->tsite, g, 0, E->npar, count, nullptr, f, Reduce{}, st);
+  if (E->npar == 1) {  // zero odd sites of the reference-layout output
+    FZeroRef z;
+    z.g = g;
+    z.out = sref(x, g);
+    z.rhs_off = 0;
+    launch_site(E->tsite, g, 1, 1, count, nullptr, z, Reduce{}, st);
+  }
+  wl_status s = check_launch(ctx, "unpack");
+  if (s != WL_OK) return s;
+  // make the caller's stream wait for the result
+  cudaEvent_t ev;
+  WL_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaEventRecord(ev, st);
+  cudaStreamWaitEvent(ctx->stream, ev, 0);
+  cudaEventDestroy(ev);
+  return WL_OK;
+}
+
+extern "C" wl_status wl_engine_retire(wl_engine* E, int slot, void* x, wl_solve_stats* stats) {
+  if (!E || !x) WL_FAIL(nullptr, WL_ERR_ARG, "null argument");
+  if (slot < 0 || slot >= E->n) WL_FAIL(E->ctx, WL_ERR_ARG, "slot index out of range");
+  wl_status s = engine_unpack(E, slot, 1, x);
+  if (s != WL_OK) return s;
+  if (stats) {
+    s = engine_stats(E, stats, slot, 1);
+    if (s != WL_OK) return s;
+  }
+  // mark idle
+  int zero = 0;
+  cudaStream_t st = engine_stream(E);
+  WL_CUDA(E->ctx, cudaMemcpyAsync(E->status + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+  WL_CUDA(E->ctx, cudaMemcpyAsync(E->active + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+  WL_CUDA(E->ctx, cudaStreamSynchronize(st));
+  return WL_OK;
+}
+
+// ------------------------------------------------------------------ solve
+struct SolveKey {
+  const wl_ctx* ctx;
+  int op, prec, n, graph;
+  bool operator<(const SolveKey& o) const {
+    return std::tie(ctx, op, prec, n, graph) < std::tie(o.ctx, o.op, o.prec, o.n, o.graph);
+  }
+};
+static std::map<SolveKey, wl_engine*> g_solve_cache;
+static std::mutex g_solve_mu;
+
+extern "C" wl_status wl_solve(wl_ctx* ctx, wl_gauge* G, const wl_solve_params* prm, const double* masses,
+                              const void* b, void* x, int nrhs, wl_solve_stats* stats) {
+  if (!ctx || !G || !prm || !masses || !b || !x) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
+  if (nrhs <= 0) WL_FAIL(ctx, WL_ERR_ARG, "nrhs must be positive");
+  wl_engine* E = nullptr;
+  SolveKey key{ctx, prm->op, prm->inner_prec, nrhs, prm->use_graph};
+  {
+    std::lock_guard<std::mutex> lk(g_solve_mu);
+    auto it = g_solve_cache.find(key);
+    if (it != g_solve_cache.end()) {
+      E = it->second;
+      g_solve_cache.erase(it);
+    }
+  }
+  if (E) {
+    E->gauge = G;  // wl_engine_step rebuilds the graph when the gauge id changed
+    E->prm = *prm;
+    if (E->prm.maxiter <= 0) E->prm.maxiter = 1000;
+    if (E->prm.check_every <= 0) E->prm.check_every = 8;
+    E->h_maxiter.assign(E->n, E->prm.maxiter);
+    if (E->gexec) {  // delta is captured by value in the scalar kernels
+      cudaGraphExecDestroy(E->gexec);
+      E->gexec = nullptr;
+      E->graph_built = false;
+    }
+  } else {
+    wl_status s = wl_engine_create(ctx, G, prm, nrhs, &E);
+    if (s != WL_OK) return s;
+  }
+  wl_status s = engine_admit_all(E, b, prm->use_x0 ? x : nullptr, masses);
+  int n_active = 1;
+  long long done_iters = 0;
+  const int chunk = E->prm.check_every;
+  while (s == WL_OK) {
+    s = wl_engine_poll(E, nullptr, &n_active);
+    if (s != WL_OK || n_active == 0) break;
+    if (done_iters > (long long)E->prm.maxiter + 2 * chunk) break;  // host-side guard
+    s = wl_engine_step(E, chunk);
+    done_iters += chunk;
+  }
+  if (s == WL_OK) s = engine_unpack(E, 0, nrhs, x);
+  std::vector<wl_solve_stats> tmp(nrhs);
+  if (s == WL_OK) s = engine_stats(E, stats ? stats : tmp.data(), 0, nrhs);
+  if (s != WL_OK) {
+    wl_engine_destroy(E);
+    return s;
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_solve_mu);
+    auto it = g_solve_cache.find(key);
+    if (it == g_solve_cache.end()) g_solve_cache[key] = E;
+    else wl_engine_destroy(E);
+  }
+  const wl_solve_stats* S = stats ? stats : tmp.data();
+  wl_status rc = WL_OK;
+  for (int i = 0; i < nrhs; ++i) {
+    if (S[i].status == ST_NAN) return WL_ERR_NAN;
+    if (S[i].status != ST_CONVERGED) rc = WL_NOT_CONVERGED;
+  }
+  if (rc != WL_OK) ctx->err = "one or more right-hand sides did not converge";
+  return rc;
+}
+
+// Release cached solve engines of a context (called before the context dies).
+extern "C" void wl_release_solve_cache(wl_ctx* ctx) {
+  std::lock_guard<std::mutex> lk(g_solve_mu);
+  for (auto it = g_solve_cache.begin(); it != g_solve_cache.end();) {
+    if (it->first.ctx == ctx) {
+      wl_engine_destroy(it->second);
+      it = g_solve_cache.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}

@@ -1,0 +1,395 @@
+// Shared device definitions for the sm_100a SU(3) Wilson-fermion library.
+//
+// Internal HBM layout (all kernels of the solver path):
+//   * even/odd "compact" site order: a site (x,y,z,t) of parity p=(x+y+z+t)&1
+//     has compact index c = flat/2 with flat = ((x*Ly+y)*Lz+z)*Lt+t.  With Lt
+//     even this equals the reference's ascending-flat-index ordering of the
+//     parity-p sites (jaxqft/models/su3_wilson_nf2.py:831-840).
+//   * spinors are structure-of-arrays per right-hand side:
+//       FP64: double2 [rhs][12][Vh]    (component k = spin*3 + colour)
+//       FP32: float4  [rhs][6][Vh]     (two complex components per float4)
+//       FP16: uint4   [rhs][3][Vh]     (eight halves = four complex) + float norm[rhs][Vh]
+//     so one warp's load of one chunk is 512 contiguous bytes.
+//   * links, split by the parity p of the site they start from:
+//       FP64/18: double2 [p][mu][9][Vh]   FP64/12: double2 [p][mu][6][Vh]
+//       FP32/12: float4  [p][mu][3][Vh]   FP16/12: uint2  [p][mu][3][Vh]
+//     12-real links keep rows 0 and 1; row 2 = conj(row0 x row1) (exact for SU(3)).
+//     Boundary phases are NOT folded into stored links; kernels apply them by
+//     index (forward hop from x_mu = L_mu-1, backward hop into x_mu = 0).
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#define WL_HD __host__ __device__ __forceinline__
+#define WL_D __device__ __forceinline__
+
+namespace wl {
+
+// ---------------------------------------------------------------- complex
+template <typename T> struct cplx { T re, im; };
+template <typename T> WL_HD cplx<T> mk(T r, T i) { return cplx<T>{r, i}; }
+template <typename T> WL_HD cplx<T> operator+(cplx<T> a, cplx<T> b) { return {a.re + b.re, a.im + b.im}; }
+template <typename T> WL_HD cplx<T> operator-(cplx<T> a, cplx<T> b) { return {a.re - b.re, a.im - b.im}; }
+template <typename T> WL_HD cplx<T> operator*(cplx<T> a, cplx<T> b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename T> WL_HD cplx<T> operator*(T s, cplx<T> a) { return {s * a.re, s * a.im}; }
+template <typename T> WL_HD cplx<T> conj(cplx<T> a) { return {a.re, -a.im}; }
+// i*a and -i*a
+template <typename T> WL_HD cplx<T> mul_i(cplx<T> a) { return {-a.im, a.re}; }
+template <typename T> WL_HD cplx<T> mul_mi(cplx<T> a) { return {a.im, -a.re}; }
+// a += b*c ; a += conj(b)*c
+template <typename T> WL_HD void fma_(cplx<T>& a, cplx<T> b, cplx<T> c) {
+  a.re += b.re * c.re - b.im * c.im;
+  a.im += b.re * c.im + b.im * c.re;
+}
+template <typename T> WL_HD void fmac_(cplx<T>& a, cplx<T> b, cplx<T> c) {
+  a.re += b.re * c.re + b.im * c.im;
+  a.im += b.re * c.im - b.im * c.re;
+}
+template <typename T> WL_HD T norm2(cplx<T> a) { return a.re * a.re + a.im * a.im; }
+
+template <typename T> struct Spinor { cplx<T> v[4][3]; };
+template <typename T> struct Half { cplx<T> v[2][3]; };
+template <typename T> struct Link { cplx<T> m[3][3]; };
+
+template <typename T> WL_D void zero(Spinor<T>& s) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) s.v[a][c] = {T(0), T(0)};
+}
+
+// ---------------------------------------------------------------- geometry
+struct Geom {
+  int L[4];      // Lx, Ly, Lz, Lt
+  int Lth;       // Lt / 2
+  int Vh;        // V / 2
+  int V;
+  int strideRow[3];  // row stride of x, y, z in units of rows: Ly*Lz, Lz, 1
+  double ph_re[4], ph_im[4];  // boundary phase per direction
+  int ph_on[4];               // phase != 1
+};
+
+struct Site {
+  int c;       // compact index
+  int row;     // (x*Ly+y)*Lz+z
+  int x[4];    // coordinates
+};
+
+WL_D Site site_from_compact(const Geom& g, int parity, int c) {
+  Site s;
+  s.c = c;
+  int th = c % g.Lth;
+  int row = c / g.Lth;
+  s.row = row;
+  s.x[2] = row % g.L[2];
+  int r2 = row / g.L[2];
+  s.x[1] = r2 % g.L[1];
+  s.x[0] = r2 / g.L[1];
+  s.x[3] = 2 * th + ((parity + s.x[0] + s.x[1] + s.x[2]) & 1);
+  return s;
+}
+
+// compact index (in the opposite-parity field) of the neighbour x + dir*e_mu
+WL_D int neighbor(const Geom& g, const Site& s, int mu, int dir) {
+  if (mu == 3) {
+    int t = s.x[3] + dir;
+    t = (t < 0) ? t + g.L[3] : (t >= g.L[3] ? t - g.L[3] : t);
+    return s.row * g.Lth + (t >> 1);
+  }
+  int xm = s.x[mu] + dir;
+  int row = s.row + dir * g.strideRow[mu];
+  if (xm < 0) row += g.L[mu] * g.strideRow[mu];
+  else if (xm >= g.L[mu]) row -= g.L[mu] * g.strideRow[mu];
+  return row * g.Lth + (s.x[3] >> 1);
+}
+
+// ---------------------------------------------------------------- loads
+WL_D double2 ldg(const double2* p) { return __ldg(p); }
+WL_D float4 ldg(const float4* p) { return __ldg(p); }
+WL_D uint4 ldg(const uint4* p) { return __ldg(p); }
+WL_D uint2 ldg(const uint2* p) { return __ldg(p); }
+WL_D float ldg(const float* p) { return __ldg(p); }
+
+WL_D float2 h2f(unsigned int u) {
+  __half2 h = *reinterpret_cast<__half2*>(&u);
+  return __half22float2(h);
+}
+WL_D unsigned int f2h(float a, float b) {
+  __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<unsigned int*>(&h);
+}
+
+// ---------------------------------------------------------------- precisions
+enum Prec { P_DOUBLE = 0, P_SINGLE = 1, P_HALF = 2 };
+
+// Spinor field in the internal SoA compact layout.
+template <int P> struct SpinorField;
+
+template <> struct SpinorField<P_DOUBLE> {
+  using real = double;
+  double2* ptr;       // [rhs][12][Vh]
+  float* norm;        // unused
+  long long rstride;  // elements (double2) per rhs
+  int vh;
+  WL_D void load(Spinor<double>& s, int rhs, int c) const {
+    const double2* b = ptr + rhs * rstride + c;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      double2 v = ldg(b + (long long)k * vh);
+      s.v[k / 3][k % 3] = {v.x, v.y};
+    }
+  }
+  WL_D void load_plain(Spinor<double>& s, int rhs, int c) const {  // for read-after-write within a kernel
+    const double2* b = ptr + rhs * rstride + c;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      double2 v = b[(long long)k * vh];
+      s.v[k / 3][k % 3] = {v.x, v.y};
+    }
+  }
+  WL_D void store(const Spinor<double>& s, int rhs, int c) const {
+    double2* b = ptr + rhs * rstride + c;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) b[(long long)k * vh] = make_double2(s.v[k / 3][k % 3].re, s.v[k / 3][k % 3].im);
+  }
+};
+
+template <> struct SpinorField<P_SINGLE> {
+  using real = float;
+  float4* ptr;  // [rhs][6][Vh]
+  float* norm;
+  long long rstride;
+  int vh;
+  WL_D void load(Spinor<float>& s, int rhs, int c) const {
+    const float4* b = ptr + rhs * rstride + c;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      float4 v = ldg(b + (long long)k * vh);
+      int i0 = 2 * k, i1 = 2 * k + 1;
+      s.v[i0 / 3][i0 % 3] = {v.x, v.y};
+      s.v[i1 / 3][i1 % 3] = {v.z, v.w};
+    }
+  }
+  WL_D void load_plain(Spinor<float>& s, int rhs, int c) const {
+    const float4* b = ptr + rhs * rstride + c;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      float4 v = b[(long long)k * vh];
+      int i0 = 2 * k, i1 = 2 * k + 1;
+      s.v[i0 / 3][i0 % 3] = {v.x, v.y};
+      s.v[i1 / 3][i1 % 3] = {v.z, v.w};
+    }
+  }
+  WL_D void store(const Spinor<float>& s, int rhs, int c) const {
+    float4* b = ptr + rhs * rstride + c;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      int i0 = 2 * k, i1 = 2 * k + 1;
+      b[(long long)k * vh] = make_float4(s.v[i0 / 3][i0 % 3].re, s.v[i0 / 3][i0 % 3].im, s.v[i1 / 3][i1 % 3].re,
+                                         s.v[i1 / 3][i1 % 3].im);
+    }
+  }
+};
+
+template <> struct SpinorField<P_HALF> {
+  using real = float;
+  uint4* ptr;   // [rhs][3][Vh]
+  float* norm;  // [rhs][Vh]
+  long long rstride;
+  int vh;
+  template <bool NC>
+  WL_D void load_impl(Spinor<float>& s, int rhs, int c) const {
+    const uint4* b = ptr + rhs * rstride + c;
+    float nrm = NC ? ldg(norm + (long long)rhs * vh + c) : norm[(long long)rhs * vh + c];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      uint4 v = NC ? ldg(b + (long long)k * vh) : b[(long long)k * vh];
+      float2 a0 = h2f(v.x), a1 = h2f(v.y), a2 = h2f(v.z), a3 = h2f(v.w);
+      int i = 4 * k;
+      s.v[(i + 0) / 3][(i + 0) % 3] = {a0.x * nrm, a0.y * nrm};
+      s.v[(i + 1) / 3][(i + 1) % 3] = {a1.x * nrm, a1.y * nrm};
+      s.v[(i + 2) / 3][(i + 2) % 3] = {a2.x * nrm, a2.y * nrm};
+      s.v[(i + 3) / 3][(i + 3) % 3] = {a3.x * nrm, a3.y * nrm};
+    }
+  }
+  WL_D void load(Spinor<float>& s, int rhs, int c) const { load_impl<true>(s, rhs, c); }
+  WL_D void load_plain(Spinor<float>& s, int rhs, int c) const { load_impl<false>(s, rhs, c); }
+  WL_D void store(const Spinor<float>& s, int rhs, int c) const {
+    float mx = 0.f;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) mx = fmaxf(mx, fmaxf(fabsf(s.v[a][cc].re), fabsf(s.v[a][cc].im)));
+    float inv = mx > 0.f ? 1.0f / mx : 0.f;
+    norm[(long long)rhs * vh + c] = mx;
+    uint4* b = ptr + rhs * rstride + c;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      int i = 4 * k;
+      const cplx<float>& c0 = s.v[(i + 0) / 3][(i + 0) % 3];
+      const cplx<float>& c1 = s.v[(i + 1) / 3][(i + 1) % 3];
+      const cplx<float>& c2 = s.v[(i + 2) / 3][(i + 2) % 3];
+      const cplx<float>& c3 = s.v[(i + 3) / 3][(i + 3) % 3];
+      uint4 v;
+      v.x = f2h(c0.re * inv, c0.im * inv);
+      v.y = f2h(c1.re * inv, c1.im * inv);
+      v.z = f2h(c2.re * inv, c2.im * inv);
+      v.w = f2h(c3.re * inv, c3.im * inv);
+      b[(long long)k * vh] = v;
+    }
+  }
+};
+
+// Spinor field in the reference layout: complex128 [rhs][V][4][3], site = flat index.
+struct SpinorRef {
+  using real = double;
+  double2* ptr;
+  long long rstride;  // double2 per rhs (= 12*V)
+  int Lt;
+  WL_D static int flat(int parity_off_unused, int c) { return c; }
+  WL_D void load(Spinor<double>& s, int rhs, long long flat) const {
+    const double2* b = ptr + rhs * rstride + flat * 12;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      double2 v = ldg(b + k);
+      s.v[k / 3][k % 3] = {v.x, v.y};
+    }
+  }
+  WL_D void store(const Spinor<double>& s, int rhs, long long flat) const {
+    double2* b = ptr + rhs * rstride + flat * 12;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) b[k] = make_double2(s.v[k / 3][k % 3].re, s.v[k / 3][k % 3].im);
+  }
+};
+
+// flat index of compact site c of the given parity
+WL_D long long flat_of(const Geom& g, int parity, int c) {
+  Site s = site_from_compact(g, parity, c);
+  return (long long)s.row * g.L[3] + s.x[3];
+}
+
+// ---------------------------------------------------------------- links
+template <typename T> WL_D void reconstruct_row2(Link<T>& u) {
+  // row2 = conj(row0 x row1)
+  u.m[2][0] = conj(u.m[0][1] * u.m[1][2] - u.m[0][2] * u.m[1][1]);
+  u.m[2][1] = conj(u.m[0][2] * u.m[1][0] - u.m[0][0] * u.m[1][2]);
+  u.m[2][2] = conj(u.m[0][0] * u.m[1][1] - u.m[0][1] * u.m[1][0]);
+}
+
+enum LinkKind { L_D18 = 0, L_D12 = 1, L_S12 = 2, L_H12 = 3, L_REF = 4 };
+
+template <int K> struct LinkField;
+
+template <> struct LinkField<L_D18> {
+  using real = double;
+  const double2* ptr;  // [p][mu][9][Vh]
+  int vh;
+  WL_D void load(Link<double>& u, int p, int mu, int c) const {
+    const double2* b = ptr + ((long long)(p * 4 + mu) * 9) * vh + c;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      double2 v = ldg(b + (long long)k * vh);
+      u.m[k / 3][k % 3] = {v.x, v.y};
+    }
+  }
+};
+
+template <> struct LinkField<L_D12> {
+  using real = double;
+  const double2* ptr;  // [p][mu][6][Vh]
+  int vh;
+  WL_D void load(Link<double>& u, int p, int mu, int c) const {
+    const double2* b = ptr + ((long long)(p * 4 + mu) * 6) * vh + c;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      double2 v = ldg(b + (long long)k * vh);
+      u.m[k / 3][k % 3] = {v.x, v.y};
+    }
+    reconstruct_row2(u);
+  }
+};
+
+template <> struct LinkField<L_S12> {
+  using real = float;
+  const float4* ptr;  // [p][mu][3][Vh]
+  int vh;
+  WL_D void load(Link<float>& u, int p, int mu, int c) const {
+    const float4* b = ptr + ((long long)(p * 4 + mu) * 3) * vh + c;
+    float4 a = ldg(b), bb = ldg(b + vh), cc = ldg(b + 2LL * vh);
+    u.m[0][0] = {a.x, a.y};
+    u.m[0][1] = {a.z, a.w};
+    u.m[0][2] = {bb.x, bb.y};
+    u.m[1][0] = {bb.z, bb.w};
+    u.m[1][1] = {cc.x, cc.y};
+    u.m[1][2] = {cc.z, cc.w};
+    reconstruct_row2(u);
+  }
+};
+
+template <> struct LinkField<L_H12> {
+  using real = float;
+  const uint2* ptr;  // [p][mu][3][Vh]
+  int vh;
+  WL_D void load(Link<float>& u, int p, int mu, int c) const {
+    const uint2* b = ptr + ((long long)(p * 4 + mu) * 3) * vh + c;
+    uint2 a = ldg(b), bb = ldg(b + vh), cc = ldg(b + 2LL * vh);
+    float2 t;
+    t = h2f(a.x); u.m[0][0] = {t.x, t.y};
+    t = h2f(a.y); u.m[0][1] = {t.x, t.y};
+    t = h2f(bb.x); u.m[0][2] = {t.x, t.y};
+    t = h2f(bb.y); u.m[1][0] = {t.x, t.y};
+    t = h2f(cc.x); u.m[1][1] = {t.x, t.y};
+    t = h2f(cc.y); u.m[1][2] = {t.x, t.y};
+    reconstruct_row2(u);
+  }
+};
+
+// Links in the reference layout BMXYIJ for one configuration: complex128 [mu][V][3][3].
+template <> struct LinkField<L_REF> {
+  using real = double;
+  const double2* ptr;
+  long long V;
+  WL_D void load_flat(Link<double>& u, int mu, long long flat) const {
+    const double2* b = ptr + ((long long)mu * V + flat) * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      double2 v = ldg(b + k);
+      u.m[k / 3][k % 3] = {v.x, v.y};
+    }
+  }
+};
+
+// ---------------------------------------------------------------- reductions
+// Deterministic block reduction of NV doubles; result valid in thread 0.
+template <int NV>
+WL_D void block_sum(double (&v)[NV], double* smem /* >= NV * 32 */) {
+  const int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
+  const int warp = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
+  const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double x = v[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    v[i] = x;
+  }
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int i = 0; i < NV; ++i) smem[i * 32 + warp] = v[i];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double x = lane < nwarps ? smem[i * 32 + lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      v[i] = x;
+    }
+  }
+}
+
+}  // namespace wl

@@ -1,0 +1,327 @@
+// Wilson hopping stencil for sm_100a.
+//
+// Computes, for every target site x of one parity (or both), and for NR
+// right-hand sides per thread that share one link stream,
+//     acc(x) = sum_mu [ (1 + cf g_mu) U_mu(x) psi(x+mu) + (1 + cb g_mu) U_mu^dag(x-mu) psi(x-mu) ]
+// with cf = -1, cb = +1 for D and cf = +1, cb = -1 for D^dag (the reference's
+// `sign` convention, jaxqft/fermions/wilson.py:228-284 with r = 1), and then
+// hands acc to an epilogue functor (xpay, CG update, residual, norms).  The
+// -1/2 of the Wilson normalisation lives in the epilogue coefficients.
+//
+// Spin projection uses the rank-2 structure of (1 +- g_mu) in the basis of
+// jaxqft/fermions/gamma.py:14-46 (g0 = s1 x s1, g1 = s1 x s2, g2 = s2 x I,
+// g3 = s3 x I):
+//   mu=0: h0 = s0 + c s3,   h1 = s1 + c s2,   rows 2,3 = ( c h1,  c h0)
+//   mu=1: h0 = s0 - ic s3,  h1 = s1 + ic s2,  rows 2,3 = (-ic h1, ic h0)
+//   mu=2: h0 = s0 - ic s2,  h1 = s1 - ic s3,  rows 2,3 = ( ic h0, ic h1)
+//   mu=3: c=+1: (2 s0, 2 s1, 0, 0);  c=-1: (0, 0, 2 s2, 2 s3)
+// so each hop multiplies the link into two colour vectors instead of four.
+#pragma once
+#include "wl_common.cuh"
+
+namespace wl {
+
+template <int MU, int C, typename T>
+WL_D void spin_project(const Spinor<T>& s, Half<T>& h) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (MU == 0) {
+      h.v[0][c] = C > 0 ? s.v[0][c] + s.v[3][c] : s.v[0][c] - s.v[3][c];
+      h.v[1][c] = C > 0 ? s.v[1][c] + s.v[2][c] : s.v[1][c] - s.v[2][c];
+    } else if (MU == 1) {
+      h.v[0][c] = C > 0 ? s.v[0][c] + mul_mi(s.v[3][c]) : s.v[0][c] + mul_i(s.v[3][c]);
+      h.v[1][c] = C > 0 ? s.v[1][c] + mul_i(s.v[2][c]) : s.v[1][c] + mul_mi(s.v[2][c]);
+    } else if (MU == 2) {
+      h.v[0][c] = C > 0 ? s.v[0][c] + mul_mi(s.v[2][c]) : s.v[0][c] + mul_i(s.v[2][c]);
+      h.v[1][c] = C > 0 ? s.v[1][c] + mul_mi(s.v[3][c]) : s.v[1][c] + mul_i(s.v[3][c]);
+    } else {
+      h.v[0][c] = C > 0 ? T(2) * s.v[0][c] : T(2) * s.v[2][c];
+      h.v[1][c] = C > 0 ? T(2) * s.v[1][c] : T(2) * s.v[3][c];
+    }
+  }
+}
+
+template <int MU, int C, typename T>
+WL_D void spin_accum(Spinor<T>& a, const Half<T>& h) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (MU == 0) {
+      a.v[0][c] = a.v[0][c] + h.v[0][c];
+      a.v[1][c] = a.v[1][c] + h.v[1][c];
+      a.v[2][c] = C > 0 ? a.v[2][c] + h.v[1][c] : a.v[2][c] - h.v[1][c];
+      a.v[3][c] = C > 0 ? a.v[3][c] + h.v[0][c] : a.v[3][c] - h.v[0][c];
+    } else if (MU == 1) {
+      a.v[0][c] = a.v[0][c] + h.v[0][c];
+      a.v[1][c] = a.v[1][c] + h.v[1][c];
+      a.v[2][c] = C > 0 ? a.v[2][c] + mul_mi(h.v[1][c]) : a.v[2][c] + mul_i(h.v[1][c]);
+      a.v[3][c] = C > 0 ? a.v[3][c] + mul_i(h.v[0][c]) : a.v[3][c] + mul_mi(h.v[0][c]);
+    } else if (MU == 2) {
+      a.v[0][c] = a.v[0][c] + h.v[0][c];
+      a.v[1][c] = a.v[1][c] + h.v[1][c];
+      a.v[2][c] = C > 0 ? a.v[2][c] + mul_i(h.v[0][c]) : a.v[2][c] + mul_mi(h.v[0][c]);
+      a.v[3][c] = C > 0 ? a.v[3][c] + mul_i(h.v[1][c]) : a.v[3][c] + mul_mi(h.v[1][c]);
+    } else {
+      if (C > 0) {
+        a.v[0][c] = a.v[0][c] + h.v[0][c];
+        a.v[1][c] = a.v[1][c] + h.v[1][c];
+      } else {
+        a.v[2][c] = a.v[2][c] + h.v[0][c];
+        a.v[3][c] = a.v[3][c] + h.v[1][c];
+      }
+    }
+  }
+}
+
+// uh = U h  (fwd) or U^dag h (bwd), both spin rows
+template <bool DAGU, typename T>
+WL_D void color_mul(const Link<T>& u, const Half<T>& h, Half<T>& o) {
+#pragma unroll
+  for (int s = 0; s < 2; ++s)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      cplx<T> acc = {T(0), T(0)};
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        if (DAGU) fmac_(acc, u.m[b][a], h.v[s][b]);
+        else fma_(acc, u.m[a][b], h.v[s][b]);
+      }
+      o.v[s][a] = acc;
+    }
+}
+
+template <typename T>
+WL_D void phase_mul(Half<T>& h, T re, T im) {
+#pragma unroll
+  for (int s = 0; s < 2; ++s)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) h.v[s][a] = h.v[s][a] * cplx<T>{re, im};
+}
+
+// Index maps: internal compact layout vs reference flat layout.
+struct IdxCompact {
+  WL_D static long long self(const Geom&, const Site& s) { return s.c; }
+  WL_D static long long nb(const Geom& g, const Site& s, int mu, int dir) { return neighbor(g, s, mu, dir); }
+};
+struct IdxFlat {
+  WL_D static long long self(const Geom& g, const Site& s) { return (long long)s.row * g.L[3] + s.x[3]; }
+  WL_D static long long nb(const Geom& g, const Site& s, int mu, int dir) {
+    int x[4] = {s.x[0], s.x[1], s.x[2], s.x[3]};
+    int v = x[mu] + dir;
+    x[mu] = v < 0 ? v + g.L[mu] : (v >= g.L[mu] ? v - g.L[mu] : v);
+    return (((long long)x[0] * g.L[1] + x[1]) * g.L[2] + x[2]) * g.L[3] + x[3];
+  }
+};
+
+// Reference-layout link field adapter with the internal load() signature.
+struct LinkRefAdapter {
+  using real = double;
+  LinkField<L_REF> f;
+  WL_D void load(Link<double>& u, int /*p*/, int mu, long long flat) const { f.load_flat(u, mu, flat); }
+};
+// Reference-layout spinor adapter
+struct SpinorRefAdapter {
+  using real = double;
+  SpinorRef f;
+  WL_D void load(Spinor<double>& s, int rhs, long long flat) const { f.load(s, rhs, flat); }
+  WL_D void load_plain(Spinor<double>& s, int rhs, long long flat) const { f.load(s, rhs, flat); }
+  WL_D void store(const Spinor<double>& s, int rhs, long long flat) const { f.store(s, rhs, flat); }
+};
+
+template <int MU, bool DAG, int NR, class IDX, class LF, class SF, typename T>
+WL_D void hop_dir(const Geom& g, const LF& links, const SF& src, int parity, const Site& s, int rhs0,
+                  const bool (&act)[NR], Spinor<T> (&acc)[NR]) {
+  constexpr int CF = DAG ? +1 : -1;
+  constexpr int CB = -CF;
+  {  // forward: U_mu(x) psi(x+mu), link stored on the target parity
+    const long long nb = IDX::nb(g, s, MU, +1);
+    Link<T> u;
+    links.load(u, parity, MU, IDX::self(g, s));
+    const bool ph = g.ph_on[MU] && (s.x[MU] == g.L[MU] - 1);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      if (!act[r]) continue;
+      Spinor<T> p;
+      src.load(p, rhs0 + r, nb);
+      Half<T> h, uh;
+      spin_project<MU, CF>(p, h);
+      color_mul<false>(u, h, uh);
+      if (ph) phase_mul(uh, T(g.ph_re[MU]), T(g.ph_im[MU]));
+      spin_accum<MU, CF>(acc[r], uh);
+    }
+  }
+  {  // backward: U_mu(x-mu)^dag psi(x-mu), link stored on the other parity
+    const long long nb = IDX::nb(g, s, MU, -1);
+    Link<T> u;
+    links.load(u, 1 - parity, MU, nb);
+    const bool ph = g.ph_on[MU] && (s.x[MU] == 0);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      if (!act[r]) continue;
+      Spinor<T> p;
+      src.load(p, rhs0 + r, nb);
+      Half<T> h, uh;
+      spin_project<MU, CB>(p, h);
+      color_mul<true>(u, h, uh);
+      if (ph) phase_mul(uh, T(g.ph_re[MU]), T(-g.ph_im[MU]));
+      spin_accum<MU, CB>(acc[r], uh);
+    }
+  }
+}
+
+// Launch-wide reduction bookkeeping: per-block partial sums per RHS, then the
+// last block to finish (atomic ticket per blockIdx.y) sums the partials in a
+// fixed order and writes result[rhs].  Deterministic run to run.
+struct Reduce {
+  double* partials;   // [nrhs][nblk]
+  unsigned* counter;  // [gridDim.y], zero at allocation, self-resetting
+  double* result;     // [nrhs]
+};
+
+constexpr int kMaxRB = 16;  // RHS per block (BY * NR)
+
+template <int NR>
+WL_D void reduce_rhs(const double (&val)[NR], const Reduce& R, int nrhs, const int* mask) {
+  __shared__ double sred[kMaxRB * 8];
+  __shared__ int s_last;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int lane = tx & 31, wx = tx >> 5, nwx = blockDim.x >> 5;
+  const int RB = blockDim.y * NR;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    double x = val[r];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sred[(ty * NR + r) * 8 + wx] = x;
+  }
+  __syncthreads();
+  const int tid = ty * blockDim.x + tx;
+  const int nblk = gridDim.x * gridDim.z;
+  const int blk = blockIdx.z * gridDim.x + blockIdx.x;
+  const int rbase = blockIdx.y * RB;
+  if (tid < RB) {
+    double x = 0.0;
+    for (int w = 0; w < nwx; ++w) x += sred[tid * 8 + w];
+    const int rhs = rbase + tid;
+    if (rhs < nrhs) R.partials[(long long)rhs * nblk + blk] = x;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) {
+    unsigned t = atomicAdd(&R.counter[blockIdx.y], 1u);
+    s_last = (t == (unsigned)nblk - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const int nth = blockDim.x * blockDim.y;
+  for (int i = 0; i < RB; ++i) {
+    const int rhs = rbase + i;
+    if (rhs >= nrhs) break;  // uniform across the block
+    double v[1] = {0.0};
+    for (int b = tid; b < nblk; b += nth) v[0] += __ldcg(&R.partials[(long long)rhs * nblk + b]);
+    block_sum<1>(v, sred);
+    if (tid == 0 && (mask == nullptr || mask[rhs] != 0)) R.result[rhs] = v[0];
+    __syncthreads();
+  }
+  if (tid == 0) R.counter[blockIdx.y] = 0;
+}
+
+// Generic launch parameters
+template <class LF, class SF, class EPI>
+struct HopArgs {
+  Geom g;
+  LF links;
+  SF src[2];        // indexed by source parity (= 1 - target parity)
+  int parity0;      // target parity of blockIdx.z == 0
+  int nrhs;
+  const int* mask;  // per-RHS gate (nullptr: all)
+  EPI epi;
+  Reduce red;
+};
+
+template <bool DAG, int NR, class IDX, class LF, class SF, class EPI>
+__global__ void __launch_bounds__(256) hop_kernel(HopArgs<LF, SF, EPI> A) {
+  using T = typename SF::real;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int parity = A.parity0 ^ blockIdx.z;
+  const int rhs0 = (blockIdx.y * blockDim.y + threadIdx.y) * NR;
+  double red[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) red[r] = 0.0;
+  if (c < A.g.Vh) {
+    bool act[NR];
+    bool any = false;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      act[r] = (rhs0 + r < A.nrhs) && (A.mask == nullptr || A.mask[rhs0 + r] != 0);
+      any |= act[r];
+    }
+    if (any) {
+      const Site s = site_from_compact(A.g, parity, c);
+      Spinor<T> acc[NR];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) zero(acc[r]);
+      const SF& src = A.src[1 - parity];
+      hop_dir<0, DAG, NR, IDX>(A.g, A.links, src, parity, s, rhs0, act, acc);
+      hop_dir<1, DAG, NR, IDX>(A.g, A.links, src, parity, s, rhs0, act, acc);
+      hop_dir<2, DAG, NR, IDX>(A.g, A.links, src, parity, s, rhs0, act, acc);
+      hop_dir<3, DAG, NR, IDX>(A.g, A.links, src, parity, s, rhs0, act, acc);
+      const long long self = IDX::self(A.g, s);
+#pragma unroll
+      for (int r = 0; r < NR; ++r)
+        if (act[r]) red[r] = A.epi(rhs0 + r, parity, self, acc[r]);
+    }
+  }
+  if (EPI::kReduce) reduce_rhs<NR>(red, A.red, A.nrhs, A.mask);
+}
+
+// ------------------------------------------------------------------ epilogues
+template <typename T>
+WL_D double snorm2(const Spinor<T>& s) {
+  double n = 0.0;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) n += (double)norm2(s.v[a][c]);
+  return n;
+}
+
+template <typename T>
+WL_D void axpby(Spinor<T>& o, T a, const Spinor<T>& x, T b, const Spinor<T>& y) {
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.v[s][c] = a * x.v[s][c] + b * y.v[s][c];
+}
+
+// out = a[rhs] * self + b[rhs] * acc, optional |out|^2 reduction.
+// self may be absent (has_self = 0).  a/b are per-RHS device arrays.
+template <class SF, bool RED>
+struct EpiXpay {
+  static constexpr bool kReduce = RED;
+  SF out[2];
+  SF self[2];
+  int has_self;
+  const double* a;  // per-RHS coefficients, or nullptr to use a0/b0
+  const double* b;
+  double a0, b0;
+  WL_D double operator()(int rhs, int parity, long long idx, Spinor<typename SF::real>& acc) const {
+    using T = typename SF::real;
+    Spinor<T> o;
+    const T bb = T(b ? b[rhs] : b0);
+    if (has_self) {
+      Spinor<T> x;
+      self[parity].load(x, rhs, idx);
+      axpby(o, T(a ? a[rhs] : a0), x, bb, acc);
+    } else {
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o.v[s][c] = bb * acc.v[s][c];
+    }
+    out[parity].store(o, rhs, idx);
+    return RED ? snorm2(o) : 0.0;
+  }
+};
+
+}  // namespace wl

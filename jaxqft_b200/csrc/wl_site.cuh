@@ -1,0 +1,380 @@
+// Site-local kernels: layout conversion (reference <-> internal), precision
+// conversion, gauge-field compression and the CG vector/scalar updates.
+#pragma once
+#include "wl_hop.cuh"
+
+namespace wl {
+
+// ------------------------------------------------------------- generic driver
+template <class F>
+struct SiteArgs {
+  int vh;
+  int parity0;
+  int nrhs;
+  const int* mask;
+  F f;
+  Reduce red;
+};
+
+template <int NR, class F>
+__global__ void __launch_bounds__(256) site_kernel(SiteArgs<F> A) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int parity = A.parity0 ^ blockIdx.z;
+  const int rhs0 = (blockIdx.y * blockDim.y + threadIdx.y) * NR;
+  double red[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    red[r] = 0.0;
+    const int rhs = rhs0 + r;
+    if (c < A.vh && rhs < A.nrhs && (A.mask == nullptr || A.mask[rhs] != 0)) red[r] = A.f(rhs, parity, c);
+  }
+  if (F::kReduce) reduce_rhs<NR>(red, A.red, A.nrhs, A.mask);
+}
+
+// -------------------------------------------------------- layout conversion
+// reference complex128 [rhs][V][4][3] -> internal compact field of parity p
+template <class SF>
+struct FPack {
+  static constexpr bool kReduce = true;  // returns |psi|^2 of the packed site (FP64 input)
+  Geom g;
+  SpinorRef in;   // in-field index = rhs - rhs_off
+  int rhs_off;
+  SF out[2];
+  WL_D double operator()(int rhs, int parity, int c) const {
+    const long long f = flat_of(g, parity, c);
+    Spinor<double> s;
+    in.load(s, rhs - rhs_off, f);
+    Spinor<typename SF::real> o;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        o.v[a][b] = {(typename SF::real)s.v[a][b].re, (typename SF::real)s.v[a][b].im};
+    out[parity].store(o, rhs, c);
+    return snorm2(s);
+  }
+};
+
+// internal FP64 compact -> reference layout (sites of that parity only)
+struct FUnpack {
+  static constexpr bool kReduce = false;
+  Geom g;
+  SpinorField<P_DOUBLE> in[2];
+  SpinorRef out;  // out-field index = rhs - rhs_off
+  int rhs_off;
+  WL_D double operator()(int rhs, int parity, int c) const {
+    const long long f = flat_of(g, parity, c);
+    Spinor<double> s;
+    in[parity].load(s, rhs, c);
+    out.store(s, rhs - rhs_off, f);
+    return 0.0;
+  }
+};
+
+// zero the reference-layout sites of one parity
+struct FZeroRef {
+  static constexpr bool kReduce = false;
+  Geom g;
+  SpinorRef out;
+  int rhs_off;
+  WL_D double operator()(int rhs, int parity, int c) const {
+    Spinor<double> z;
+    zero(z);
+    out.store(z, rhs - rhs_off, flat_of(g, parity, c));
+    return 0.0;
+  }
+};
+
+// precision conversion between internal compact fields, with |src|^2
+template <class SFI, class SFO>
+struct FConvert {
+  static constexpr bool kReduce = true;
+  SFI in[2];
+  SFO out[2];
+  WL_D double operator()(int rhs, int parity, int c) const {
+    Spinor<typename SFI::real> s;
+    in[parity].load_plain(s, rhs, c);
+    Spinor<typename SFO::real> o;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        o.v[a][b] = {(typename SFO::real)s.v[a][b].re, (typename SFO::real)s.v[a][b].im};
+    out[parity].store(o, rhs, c);
+    return snorm2(s);
+  }
+};
+
+// zero an internal field
+template <class SF>
+struct FZero {
+  static constexpr bool kReduce = false;
+  SF out[2];
+  WL_D double operator()(int rhs, int parity, int c) const {
+    Spinor<typename SF::real> z;
+    zero(z);
+    out[parity].store(z, rhs, c);
+    return 0.0;
+  }
+};
+
+// ------------------------------------------------------------ CG updates
+// x64 += xs (converted); xs = 0.  Gated by the reliable-update mask.
+template <class SFS>
+struct FAccumX {
+  static constexpr bool kReduce = false;
+  SpinorField<P_DOUBLE> x[2];
+  SFS xs[2];
+  WL_D double operator()(int rhs, int parity, int c) const {
+    Spinor<typename SFS::real> s;
+    xs[parity].load_plain(s, rhs, c);
+    Spinor<double> xv;
+    x[parity].load_plain(xv, rhs, c);
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        xv.v[a][b].re += (double)s.v[a][b].re;
+        xv.v[a][b].im += (double)s.v[a][b].im;
+      }
+    x[parity].store(xv, rhs, c);
+    Spinor<typename SFS::real> z;
+    zero(z);
+    xs[parity].store(z, rhs, c);
+    return 0.0;
+  }
+};
+
+// p = rs + beta * p.  Gated by the active mask.
+template <class SFS>
+struct FUpdateP {
+  static constexpr bool kReduce = false;
+  SFS rs[2];
+  SFS p[2];
+  const double* beta;
+  WL_D double operator()(int rhs, int parity, int c) const {
+    using T = typename SFS::real;
+    Spinor<T> r, pv, o;
+    rs[parity].load_plain(r, rhs, c);
+    p[parity].load_plain(pv, rhs, c);
+    axpby(o, T(1), r, T(beta[rhs]), pv);
+    p[parity].store(o, rhs, c);
+    return 0.0;
+  }
+};
+
+// ------------------------------------------------------------ CG epilogues
+// Last hop of the sloppy normal operator fused with the CG update:
+//   Ap = a*y + b*acc ; alpha = r2/pAp ; xs += alpha p ; rs -= alpha Ap ; return |rs|^2
+template <class SF>
+struct EpiCG {
+  static constexpr bool kReduce = true;
+  SF y[2], p[2], xs[2], rs[2];
+  const double* a;
+  const double* b;
+  const double* r2;
+  const double* pAp;
+  WL_D double operator()(int rhs, int parity, long long idx, Spinor<typename SF::real>& acc) const {
+    using T = typename SF::real;
+    const double den = pAp[rhs];
+    const T alpha = (den > 0.0) ? T(r2[rhs] / den) : T(0);
+    Spinor<T> yv, pv, xv, rv;
+    y[parity].load(yv, rhs, idx);
+    p[parity].load_plain(pv, rhs, idx);
+    xs[parity].load_plain(xv, rhs, idx);
+    rs[parity].load_plain(rv, rhs, idx);
+    const T aa = T(a[rhs]), bb = T(b[rhs]);
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cplx<T> ap = aa * yv.v[s][c] + bb * acc.v[s][c];
+        xv.v[s][c] = xv.v[s][c] + alpha * pv.v[s][c];
+        rv.v[s][c] = rv.v[s][c] - alpha * ap;
+      }
+    xs[parity].store(xv, rhs, idx);
+    rs[parity].store(rv, rhs, idx);
+    return snorm2(rv);
+  }
+};
+
+// Last hop of the FP64 normal operator on x64, giving the true residual:
+//   r = bvec - (a*y + b*acc) ; rs = convert(r) ; return |r|^2 (FP64)
+template <class SFS>
+struct EpiResid {
+  static constexpr bool kReduce = true;
+  SpinorField<P_DOUBLE> y[2], bvec[2];
+  SFS rs[2];
+  const double* a;
+  const double* b;
+  WL_D double operator()(int rhs, int parity, long long idx, Spinor<double>& acc) const {
+    Spinor<double> yv, bv;
+    y[parity].load(yv, rhs, idx);
+    bvec[parity].load(bv, rhs, idx);
+    const double aa = a[rhs], bb = b[rhs];
+    Spinor<typename SFS::real> o;
+    double n = 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cplx<double> r = bv.v[s][c] - (aa * yv.v[s][c] + bb * acc.v[s][c]);
+        n += norm2(r);
+        o.v[s][c] = {(typename SFS::real)r.re, (typename SFS::real)r.im};
+      }
+    rs[parity].store(o, rhs, idx);
+    return n;
+  }
+};
+
+// ------------------------------------------------------------ gauge upload
+// Reference BMXYIJ complex128 [mu][V][3][3] (one configuration) -> internal
+// parity-split copies.  Also records max |U U^dag - 1| + |det U - 1| so the
+// host knows whether 12-real reconstruction is exact for these links.
+struct GaugeOut {
+  double2* d18;   // [p][mu][9][Vh]
+  double2* d12;   // [p][mu][6][Vh]
+  float4* s12;    // [p][mu][3][Vh]
+  uint2* h12;     // [p][mu][3][Vh]
+  unsigned int* unitarity_err;  // float bits, atomicMax
+};
+
+__global__ void gauge_convert_kernel(Geom g, const double2* __restrict__ U, GaugeOut o) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int parity = blockIdx.y;
+  const int mu = blockIdx.z;
+  if (c >= g.Vh) return;
+  const long long f = flat_of(g, parity, c);
+  const double2* src = U + ((long long)mu * g.V + f) * 9;
+  Link<double> u;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    double2 v = src[k];
+    u.m[k / 3][k % 3] = {v.x, v.y};
+  }
+  const long long base = (long long)(parity * 4 + mu);
+  const int vh = g.Vh;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) o.d18[(base * 9 + k) * vh + c] = make_double2(u.m[k / 3][k % 3].re, u.m[k / 3][k % 3].im);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) o.d12[(base * 6 + k) * vh + c] = make_double2(u.m[k / 3][k % 3].re, u.m[k / 3][k % 3].im);
+  float f12[12];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    f12[2 * k] = (float)u.m[k / 3][k % 3].re;
+    f12[2 * k + 1] = (float)u.m[k / 3][k % 3].im;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    o.s12[(base * 3 + k) * vh + c] = make_float4(f12[4 * k], f12[4 * k + 1], f12[4 * k + 2], f12[4 * k + 3]);
+    o.h12[(base * 3 + k) * vh + c] = make_uint2(f2h(f12[4 * k], f12[4 * k + 1]), f2h(f12[4 * k + 2], f12[4 * k + 3]));
+  }
+  // unitarity / determinant check
+  double err = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      cplx<double> s = {0.0, 0.0};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) fmac_(s, u.m[j][k], u.m[i][k]);  // (U U^dag)_ij = sum_k U_ik conj(U_jk)
+      if (i == j) s.re -= 1.0;
+      err = fmax(err, sqrt(norm2(s)));
+    }
+  cplx<double> det = u.m[0][0] * (u.m[1][1] * u.m[2][2] - u.m[1][2] * u.m[2][1]) -
+                     u.m[0][1] * (u.m[1][0] * u.m[2][2] - u.m[1][2] * u.m[2][0]) +
+                     u.m[0][2] * (u.m[1][0] * u.m[2][1] - u.m[1][1] * u.m[2][0]);
+  det.re -= 1.0;
+  err = fmax(err, sqrt(norm2(det)));
+  float ef = (float)err;
+  // warp max then one atomic per warp
+  for (int off = 16; off > 0; off >>= 1) ef = fmaxf(ef, __shfl_down_sync(0xffffffffu, ef, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(o.unitarity_err, __float_as_uint(ef));
+}
+
+// ------------------------------------------------------------ scalar control
+// One block; thread s handles slot s.  See the engine for the state machine.
+struct CGScalars {
+  double* r2;        // current residual^2 used by alpha
+  double* r2_new;    // sloppy residual^2 after the update (reduction target)
+  double* pAp;       // |M p|^2 (reduction target)
+  double* r2_true;   // true residual^2 from the reliable update (reduction target)
+  double* rmax2;     // max residual^2 since the last reliable update
+  double* b2;
+  double* tol2;
+  double* beta;
+  int* active;
+  int* ru;
+  int* iters;
+  int* maxiter;
+  int* status;
+  int* n_ru;
+  int* n_active;     // single int
+  double delta2;
+};
+
+enum SlotStatus { ST_IDLE = 0, ST_RUNNING = 1, ST_CONVERGED = 2, ST_MAXITER = 3, ST_BREAKDOWN = 4, ST_NAN = 5 };
+
+__global__ void cg_decide_kernel(CGScalars S, int n) {
+  for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    S.ru[s] = 0;
+    if (!S.active[s]) continue;
+    const double r2n = S.r2_new[s];
+    const double pap = S.pAp[s];
+    if (!isfinite(r2n) || !isfinite(pap)) {
+      S.status[s] = ST_NAN;
+      S.active[s] = 0;
+      continue;
+    }
+    if (!(pap > 0.0)) {
+      S.status[s] = ST_BREAKDOWN;
+      S.active[s] = 0;
+      continue;
+    }
+    const bool trig = (r2n < S.delta2 * S.rmax2[s]) || (r2n <= S.tol2[s] * S.b2[s]) || (S.iters[s] + 1 >= S.maxiter[s]);
+    S.ru[s] = trig ? 1 : 0;
+  }
+}
+
+__global__ void cg_finalize_kernel(CGScalars S, int n) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  int local = 0;
+  for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    if (!S.active[s]) continue;
+    double r2n;
+    if (S.ru[s]) {
+      r2n = S.r2_true[s];
+      S.rmax2[s] = r2n;
+      S.n_ru[s] += 1;
+    } else {
+      r2n = S.r2_new[s];
+      S.rmax2[s] = fmax(S.rmax2[s], r2n);
+    }
+    S.iters[s] += 1;
+    if (!isfinite(r2n)) {
+      S.status[s] = ST_NAN;
+      S.active[s] = 0;
+      continue;
+    }
+    S.beta[s] = r2n / S.r2[s];
+    S.r2[s] = r2n;
+    if (S.ru[s] && r2n <= S.tol2[s] * S.b2[s]) {
+      S.status[s] = ST_CONVERGED;
+      S.active[s] = 0;
+      continue;
+    }
+    if (S.iters[s] >= S.maxiter[s]) {
+      S.status[s] = ST_MAXITER;
+      S.active[s] = 0;
+      continue;
+    }
+    local++;
+  }
+  atomicAdd(&cnt, local);
+  __syncthreads();
+  if (threadIdx.x == 0) *S.n_active = cnt;
+}
+
+}  // namespace wl

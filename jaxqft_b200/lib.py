@@ -1,0 +1,362 @@
+"""ctypes binding of libwilson_sm100.so (the C-ABI in include/wilson_sm100.h).
+
+There is no CPU fallback: every compute entry point requires the in-tree CUDA
+library and a CUDA device, and raises ``RuntimeError`` otherwise.  Field
+arguments are torch CUDA tensors (complex128, contiguous) whose device
+pointers are handed to the library; ownership stays with the caller.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwilson_sm100.so")
+HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "wilson_sm100.h")
+
+# status codes (wl_status)
+WL_OK, WL_ERR_ARG, WL_ERR_OOM, WL_NOT_CONVERGED, WL_ERR_NAN, WL_ERR_TIMEOUT, WL_ERR_CUDA, WL_ERR_STATE = range(8)
+STATUS_NAMES = {
+    WL_OK: "OK", WL_ERR_ARG: "ERR_ARG", WL_ERR_OOM: "ERR_OOM", WL_NOT_CONVERGED: "NOT_CONVERGED",
+    WL_ERR_NAN: "ERR_NAN", WL_ERR_TIMEOUT: "ERR_TIMEOUT", WL_ERR_CUDA: "ERR_CUDA", WL_ERR_STATE: "ERR_STATE",
+}
+PREC = {"double": 0, "single": 1, "half": 2, "fp64": 0, "fp32": 1, "fp16": 2}
+OPS = dict(D=0, DDAG=1, DDAGD=2, HOP=3, HOP_DAG=4, K_OE=5, K_EO=6, KDAG_OE=7, KDAG_EO=8,
+           SCHUR_E=9, SCHUR_E_DAG=10, SCHUR_O=11, SCHUR_E_NORMAL=12)
+FLAG_NORMALIZED = 1
+SOLVE_NORMAL, SOLVE_EO_NORMAL = 0, 1
+# per-RHS solver status (wl_solve_stats.status)
+SLOT_CONVERGED, SLOT_MAXITER, SLOT_BREAKDOWN, SLOT_NAN = 2, 3, 4, 5
+
+# Every symbol the header declares (checked by tests/test_abi.py).
+EXPORTS = (
+    "wl_version", "wl_ctx_create", "wl_ctx_destroy", "wl_last_error", "wl_ctx_set_stream",
+    "wl_ctx_synchronize", "wl_eo_maps", "wl_gauge_create", "wl_gauge_update", "wl_gauge_unitarity",
+    "wl_gauge_destroy", "wl_apply", "wl_solve", "wl_engine_create", "wl_engine_destroy", "wl_engine_admit",
+    "wl_engine_step", "wl_engine_poll", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
+)
+
+
+class WLGeometry(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_int * 4), ("bc_re", ctypes.c_double * 4), ("bc_im", ctypes.c_double * 4)]
+
+
+class WLSolveParams(ctypes.Structure):
+    _fields_ = [
+        ("op", ctypes.c_int), ("inner_prec", ctypes.c_int), ("tol", ctypes.c_double), ("maxiter", ctypes.c_int),
+        ("delta", ctypes.c_double), ("use_x0", ctypes.c_int), ("use_graph", ctypes.c_int),
+        ("check_every", ctypes.c_int),
+    ]
+
+
+class WLSolveStats(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int), ("reliable_updates", ctypes.c_int), ("status", ctypes.c_int),
+                ("true_res", ctypes.c_double)]
+
+
+_lib = None
+
+
+def load_library(path: Optional[str] = None) -> ctypes.CDLL:
+    """Load (and declare prototypes of) the in-tree CUDA library.  Builds it
+    with nvcc first if it is missing and a toolkit is present."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        from . import build as _build
+
+        _build.build()
+    if not os.path.exists(path):
+        raise RuntimeError(f"libwilson_sm100.so not found at {path}; run python -m jaxqft_b200.build")
+    lib = ctypes.CDLL(path)
+    vp, i, d, u = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_uint
+    pi, pd = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "wl_version": (i, []),
+        "wl_ctx_create": (i, [ctypes.POINTER(WLGeometry), i, ctypes.POINTER(vp)]),
+        "wl_ctx_destroy": (None, [vp]),
+        "wl_last_error": (ctypes.c_char_p, [vp]),
+        "wl_ctx_set_stream": (i, [vp, vp]),
+        "wl_ctx_synchronize": (i, [vp]),
+        "wl_eo_maps": (i, [vp, vp, vp, vp]),
+        "wl_gauge_create": (i, [vp, vp, ctypes.POINTER(vp)]),
+        "wl_gauge_update": (i, [vp, vp]),
+        "wl_gauge_unitarity": (i, [vp, pd]),
+        "wl_gauge_destroy": (None, [vp]),
+        "wl_apply": (i, [vp, vp, i, d, u, vp, vp, i]),
+        "wl_solve": (i, [vp, vp, ctypes.POINTER(WLSolveParams), pd, vp, vp, i, ctypes.POINTER(WLSolveStats)]),
+        "wl_engine_create": (i, [vp, vp, ctypes.POINTER(WLSolveParams), i, ctypes.POINTER(vp)]),
+        "wl_engine_destroy": (None, [vp]),
+        "wl_engine_admit": (i, [vp, pi, i, vp, pd, pd, pi]),
+        "wl_engine_step": (i, [vp, i]),
+        "wl_engine_poll": (i, [vp, pi, pi]),
+        "wl_engine_retire": (i, [vp, i, vp, ctypes.POINTER(WLSolveStats)]),
+        "wl_engine_bytes": (ctypes.c_int64, [vp, i, i, i]),
+        "wl_pf_force": (i, [vp, vp, vp, vp, d, i, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class WilsonError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _require_cuda():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("the B200 Wilson-fermion path requires a CUDA device (no CPU fallback)")
+    return torch
+
+
+def _ptr(t) -> int:
+    return int(t.data_ptr())
+
+
+def _c128(t, device):
+    import torch
+
+    if isinstance(t, np.ndarray):
+        t = torch.from_numpy(np.ascontiguousarray(t))
+    if t.dtype != torch.complex128:
+        t = t.to(torch.complex128)
+    if t.device != device:
+        t = t.to(device)
+    return t.contiguous()
+
+
+class Gauge:
+    """Device copies of one gauge configuration (internal parity-split FP64 /
+    FP32 / FP16 layouts built by the library)."""
+
+    def __init__(self, ctx: "WilsonContext", U):
+        self.ctx = ctx
+        lib = ctx.lib
+        U = _c128(U, ctx.device)
+        h = ctypes.c_void_p()
+        ctx._check(lib.wl_gauge_create(ctx.handle, _ptr(U), ctypes.byref(h)))
+        self.handle = h
+        self._src = U  # keep the source alive until the async copy has run
+
+    def update(self, U):
+        U = _c128(U, self.ctx.device)
+        self.ctx._check(self.ctx.lib.wl_gauge_update(self.handle, _ptr(U)))
+        self._src = U
+
+    def unitarity(self) -> float:
+        v = ctypes.c_double()
+        self.ctx._check(self.ctx.lib.wl_gauge_unitarity(self.handle, ctypes.byref(v)))
+        return float(v.value)
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.ctx.lib.wl_gauge_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class WilsonContext:
+    """One lattice geometry on one CUDA device (wraps wl_ctx)."""
+
+    def __init__(self, lattice_shape: Sequence[int], bc=(1, 1, 1, 1), device=None):
+        torch = _require_cuda()
+        self.lib = load_library()
+        if len(lattice_shape) != 4:
+            raise ValueError("the SU(3) Wilson path is 4-dimensional")
+        self.lattice_shape = tuple(int(v) for v in lattice_shape)
+        if any(v < 2 or v % 2 for v in self.lattice_shape):
+            raise ValueError("every lattice extent must be even and >= 2 (even/odd layout)")
+        self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.volume = int(np.prod(self.lattice_shape))
+        g = WLGeometry()
+        for mu in range(4):
+            g.dims[mu] = self.lattice_shape[mu]
+            p = complex(bc[mu])
+            g.bc_re[mu] = p.real
+            g.bc_im[mu] = p.imag
+        h = ctypes.c_void_p()
+        rc = self.lib.wl_ctx_create(ctypes.byref(g), int(self.device.index or 0), ctypes.byref(h))
+        if rc != WL_OK:
+            raise WilsonError(rc, self.lib.wl_last_error(None).decode())
+        self.handle = h
+        self.bc = tuple(complex(b) for b in bc)
+        self.set_stream(torch.cuda.current_stream(self.device))
+
+    def set_stream(self, stream):
+        self._check(self.lib.wl_ctx_set_stream(self.handle, ctypes.c_void_p(int(stream.cuda_stream))))
+
+    def _check(self, rc: int):
+        if rc != WL_OK:
+            raise WilsonError(rc, self.lib.wl_last_error(self.handle).decode())
+
+    def gauge(self, U) -> Gauge:
+        return Gauge(self, U)
+
+    def synchronize(self):
+        self._check(self.lib.wl_ctx_synchronize(self.handle))
+
+    # ------------------------------------------------------------ operators
+    def apply(self, op: str, gauge: Gauge, mass: float, psi, normalized: bool = False, out=None):
+        """out = op(psi) for psi of shape (nrhs, Lx, Ly, Lz, Lt, 4, 3) or (Lx..Lt, 4, 3)."""
+        import torch
+
+        psi = _c128(psi, self.device)
+        nrhs = psi.numel() // (12 * self.volume)
+        if nrhs * 12 * self.volume != psi.numel():
+            raise ValueError(f"field of {psi.numel()} elements does not match lattice {self.lattice_shape}")
+        if out is None:
+            out = torch.empty_like(psi)
+        flags = FLAG_NORMALIZED if normalized else 0
+        self._check(self.lib.wl_apply(self.handle, gauge.handle, OPS[op], float(mass), flags, _ptr(psi), _ptr(out),
+                                      nrhs))
+        return out
+
+    def pf_force(self, gauge: Gauge, X, Y, coef: float = 1.0, F=None):
+        """F (+)= coef * pseudofermion_force_from_solution(U, X, Y) for one configuration."""
+        import torch
+
+        X = _c128(X, self.device)
+        Y = _c128(Y, self.device)
+        acc = F is not None
+        if F is None:
+            F = torch.empty((4, *self.lattice_shape, 3, 3), dtype=torch.complex128, device=self.device)
+        self._check(self.lib.wl_pf_force(self.handle, gauge.handle, _ptr(X), _ptr(Y), float(coef), int(acc),
+                                         _ptr(F)))
+        return F
+
+    def eo_maps(self):
+        vh = self.volume // 2
+        even = np.zeros(vh, dtype=np.int32)
+        odd = np.zeros(vh, dtype=np.int32)
+        nbr = np.zeros((2, 4, 2, vh), dtype=np.int32)
+        self._check(self.lib.wl_eo_maps(self.handle, even.ctypes.data, odd.ctypes.data, nbr.ctypes.data))
+        return even, odd, nbr
+
+    # ------------------------------------------------------------ solves
+    def solve(self, gauge: Gauge, b, masses, op: str = "eo_normal", tol: float = 1e-10, maxiter: int = 1000,
+              inner: str = "double", delta: float = 0.1, x0=None, use_graph: bool = True, check_every: int = 8):
+        """Batched CG for nrhs systems sharing `gauge`.  Returns (x, stats list)."""
+        import torch
+
+        b = _c128(b, self.device)
+        nrhs = b.numel() // (12 * self.volume)
+        masses = np.broadcast_to(np.asarray(masses, dtype=np.float64), (nrhs,)).copy()
+        if x0 is not None:
+            x = _c128(x0, self.device).clone()
+        else:
+            x = torch.empty_like(b)
+        p = WLSolveParams()
+        p.op = SOLVE_EO_NORMAL if op == "eo_normal" else SOLVE_NORMAL
+        p.inner_prec = PREC[inner]
+        p.tol = float(tol)
+        p.maxiter = int(maxiter)
+        p.delta = float(delta if inner != "double" else 0.0)
+        p.use_x0 = int(x0 is not None)
+        p.use_graph = int(bool(use_graph))
+        p.check_every = int(check_every)
+        stats = (WLSolveStats * nrhs)()
+        rc = self.lib.wl_solve(self.handle, gauge.handle, ctypes.byref(p),
+                               masses.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _ptr(b), _ptr(x), nrhs, stats)
+        st = [dict(iters=s.iters, reliable_updates=s.reliable_updates, status=s.status, true_res=s.true_res)
+              for s in stats]
+        if rc not in (WL_OK, WL_NOT_CONVERGED):
+            self._check(rc)
+        return x, st
+
+    def engine_bytes(self, op: str, inner: str, nslots: int) -> int:
+        return int(self.lib.wl_engine_bytes(self.handle, SOLVE_EO_NORMAL if op == "eo_normal" else SOLVE_NORMAL,
+                                            PREC[inner], int(nslots)))
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.lib.wl_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Engine:
+    """Continuous-batching CG engine (wl_engine): fixed RHS slots on one gauge."""
+
+    def __init__(self, ctx: WilsonContext, gauge: Gauge, nslots: int, op: str = "eo_normal", inner: str = "half",
+                 tol: float = 1e-10, maxiter: int = 2000, delta: float = 0.1, use_graph: bool = True):
+        self.ctx, self.gauge, self.nslots = ctx, gauge, int(nslots)
+        p = WLSolveParams()
+        p.op = SOLVE_EO_NORMAL if op == "eo_normal" else SOLVE_NORMAL
+        p.inner_prec = PREC[inner]
+        p.tol = float(tol)
+        p.maxiter = int(maxiter)
+        p.delta = float(delta if inner != "double" else 0.0)
+        p.use_graph = int(bool(use_graph))
+        p.check_every = 8
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.wl_engine_create(ctx.handle, gauge.handle, ctypes.byref(p), self.nslots, ctypes.byref(h)))
+        self.handle = h
+        self._inputs = []
+
+    def admit(self, slots, b, masses, tols=None, maxiters=None):
+        b = _c128(b, self.ctx.device)
+        slots = np.ascontiguousarray(slots, dtype=np.int32)
+        n = slots.size
+        masses = np.broadcast_to(np.asarray(masses, dtype=np.float64), (n,)).copy()
+        tp = None if tols is None else np.broadcast_to(np.asarray(tols, np.float64), (n,)).copy()
+        mp = None if maxiters is None else np.broadcast_to(np.asarray(maxiters, np.int32), (n,)).copy()
+        self.ctx._check(self.ctx.lib.wl_engine_admit(
+            self.handle, slots.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n, _ptr(b),
+            masses.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            None if tp is None else tp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            None if mp is None else mp.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self._inputs.append(b)
+
+    def step(self, iters: int):
+        self.ctx._check(self.ctx.lib.wl_engine_step(self.handle, int(iters)))
+
+    def poll(self):
+        st = np.zeros(self.nslots, dtype=np.int32)
+        na = ctypes.c_int()
+        self.ctx._check(self.ctx.lib.wl_engine_poll(self.handle, st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                    ctypes.byref(na)))
+        self._inputs = []
+        return st, int(na.value)
+
+    def retire(self, slot: int, out=None):
+        import torch
+
+        if out is None:
+            out = torch.empty((*self.ctx.lattice_shape, 4, 3), dtype=torch.complex128, device=self.ctx.device)
+        s = WLSolveStats()
+        self.ctx._check(self.ctx.lib.wl_engine_retire(self.handle, int(slot), _ptr(out), ctypes.byref(s)))
+        return out, dict(iters=s.iters, reliable_updates=s.reliable_updates, status=s.status, true_res=s.true_res)
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.ctx.lib.wl_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
