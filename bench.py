@@ -1,0 +1,400 @@
+#!/usr/bin/env python
+"""Benchmark: batched mixed-precision Wilson CG solves/s on 24^3x48 (B200).
+
+Workload (one "step"): the even-odd preconditioned Wilson normal system
+(M^dag M) x_e = b_e of jaxQFT's solve_eop_even_normal on a 24^3x48 lattice,
+kappa = 0.135 (bare mass 1/(2 kappa) - 4), antiperiodic time boundary,
+links exp(i*0.2*H) per link (H traceless Hermitian, Gaussian entries), and
+16 right-hand sides -- 12 point sources (one per spin x colour at site 0) and
+4 Gaussian spinors, each passed through M^dag as the propagator code passes
+its sources through D^dag.  All 16 are solved in ONE batched CG whose inner
+operator runs in FP16 storage / FP32 arithmetic with FP64 reliable updates,
+to an FP64 true residual ||b - M^dag M x|| / ||b|| <= 1e-10 for every RHS.
+
+Reported: value = solves/s of that batched mixed solve (device time, CUDA
+events on the solver stream, inputs resident in HBM), next to plain FP64 CG
+(one RHS at a time) on the same systems; e2e = the same solve through the
+public API from pinned host buffers with host<->device copies timed; the
+roofline of the dominant kernel (the FP16 16-RHS hop) measured live; and a
+CPU baseline (the C restatement of the reference's CG on the host cores).
+
+Data is synthetic (seeded); every working set is larger than the 126 MB L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (24, 24, 24, 48)
+KAPPA = 0.135
+MASS = 1.0 / (2.0 * KAPPA) - 4.0
+BC = (1, 1, 1, -1)
+LINK_SCALE = 0.2
+NRHS = 16
+TOL = 1e-10
+METRIC = "CG solves/s 24^3x48 mixed vs FP64 @1e-10; Dslash HBM GB/s; serve p50/p99 ms"
+WORKLOAD = ("EO-preconditioned Wilson normal-equation CG (solve_eop_even_normal), 24^3x48, kappa 0.135, "
+            "antiperiodic t, links exp(i*0.2*H), 16 RHS (12 point sources at site 0 + 4 Gaussian) in one batched "
+            "FP16/FP32 CG with FP64 reliable updates, true residual 1e-10")
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(key: str):
+    """Per-launch DRAM bytes of the dominant kernel from a committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == key:
+            return float(parts[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    f = [v.strip() for v in line.split(",")]
+                    if len(f) >= 9:
+                        self.samples.append(f)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# --------------------------------------------------------------------------- inputs
+def make_inputs(torch, device, seed: int):
+    """Links exp(TA(a (G1 + i G2))) (= exp(i a H)) and the 16 raw sources."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    shp = (4, *SHAPE, 3, 3)
+    A = LINK_SCALE * torch.complex(torch.randn(shp, generator=g, device=device, dtype=torch.float64),
+                                   torch.randn(shp, generator=g, device=device, dtype=torch.float64))
+    Y = 0.5 * (A - A.conj().transpose(-1, -2))
+    del A
+    tr = torch.diagonal(Y, dim1=-2, dim2=-1).sum(-1) / 3.0
+    Y = Y - tr[..., None, None] * torch.eye(3, device=device, dtype=Y.dtype)
+    U = torch.linalg.matrix_exp(Y)
+    del Y
+    eta = torch.zeros((NRHS, *SHAPE, 4, 3), dtype=torch.complex128, device=device)
+    for k in range(12):  # point sources at site 0 (an even site)
+        eta[k, 0, 0, 0, 0, k // 3, k % 3] = 1.0
+    fshape = (NRHS - 12, *SHAPE, 4, 3)
+    eta[12:] = torch.complex(torch.randn(fshape, generator=g, device=device, dtype=torch.float64),
+                             torch.randn(fshape, generator=g, device=device, dtype=torch.float64)) / np.sqrt(2.0)
+    return U, eta
+
+
+def even_mask(torch, device):
+    x = [torch.arange(n, device=device) for n in SHAPE]
+    par = (x[0][:, None, None, None] + x[1][None, :, None, None] + x[2][None, None, :, None]
+           + x[3][None, None, None, :]) % 2
+    return (par == 0).to(torch.complex128)[..., None, None]
+
+
+# --------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+
+    from jaxqft_b200 import lib as L
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    ctx = L.WilsonContext(SHAPE, bc=BC, device=dev)
+    U, eta = make_inputs(torch, dev, seed=rank)
+    gauge = ctx.gauge(U)
+    # b_e = M^dag eta_e  (normalized Schur dagger, even sites)
+    b = ctx.apply("SCHUR_E_DAG", gauge, MASS, eta * even_mask(torch, dev), normalized=True)
+    torch.cuda.synchronize()
+
+    eng = L.Engine(ctx, gauge, NRHS, op="eo_normal", inner="half", tol=TOL, maxiter=4000, delta=0.1)
+    estream = eng.stream
+    x = torch.empty_like(b)
+    slots = np.arange(NRHS)
+
+    def batched_solve(engine, bb, xx, n):
+        engine.admit(np.arange(n), bb, MASS)
+        na = n
+        while na > 0:
+            engine.step(8)
+            st, na = engine.poll()
+        stats = []
+        for s in range(n):
+            _, info = engine.retire(s, out=xx[s])
+            stats.append(info)
+        return stats
+
+    def timed(fn, stream):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, out
+
+    # warm-up (graph capture, autotune, first-touch)
+    for _ in range(args.warmup):
+        stats = batched_solve(eng, b, x, NRHS)
+    launches0 = L.kernel_launches()
+    times, all_stats = [], []
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t, stats = timed(lambda: batched_solve(eng, b, x, NRHS), estream)
+            times.append(t)
+            all_stats.append(stats)
+    torch.cuda.synchronize()
+    launches = L.kernel_launches() - launches0
+    t_step = float(np.mean(times))
+    t_max = t_step
+    if dist is not None:
+        tt = torch.tensor([t_step], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * NRHS / t_max
+    iters = [s["iters"] for s in all_stats[-1]]
+    res = max(s["true_res"] for st in all_stats for s in st)
+    conv = all(s["status"] == 2 for st in all_stats for s in st)
+
+    # ---- plain FP64 CG baseline: one RHS at a time, same systems
+    eng64 = L.Engine(ctx, gauge, 1, op="eo_normal", inner="double", tol=TOL, maxiter=4000)
+    batched_solve(eng64, b[12:13], x[12:13], 1)  # warm-up
+    t64, it64 = 0.0, []
+    n64 = NRHS if args.fp64_all else 4
+    for r in range(NRHS - n64, NRHS):
+        t, st = timed(lambda r=r: batched_solve(eng64, b[r:r + 1], x[r:r + 1], 1), eng64.stream)
+        t64 += t
+        it64.append(st[0]["iters"])
+    fp64_sps = n64 / t64
+    eng64.close()
+
+    # ---- live roofline of the dominant kernel (FP16 hop over 16 RHS)
+    hop_ms, hop_bytes = eng.time_hop(reps=20)
+    hbm, peak_kind = peaks()
+    achieved = hop_bytes / (hop_ms * 1e-3) / 1e9
+    traffic = profile_traffic(f"hop_h12_half_nrhs{NRHS}_{'x'.join(map(str, SHAPE))}")
+
+    # ---- e2e through the public API from pinned host buffers
+    e2e = None
+    if rank == 0 or True:
+        b_host = b.cpu().pin_memory()
+        x_host = torch.empty_like(b_host).pin_memory()
+        cur = torch.cuda.current_stream(dev)
+
+        def e2e_once():
+            bd = b_host.to(dev, non_blocking=True)
+            xd, st = ctx.solve(gauge, bd, MASS, op="eo_normal", tol=TOL, maxiter=4000, inner="half")
+            x_host.copy_(xd, non_blocking=True)
+            return st
+
+        e2e_once()
+        te = []
+        for _ in range(max(1, min(args.steps, 3))):
+            t, st = timed(e2e_once, cur)
+            te.append(t)
+        tmax = float(np.mean(te))
+        if dist is not None:
+            tt = torch.tensor([tmax], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            tmax = float(tt.item())
+        nbytes = b_host.numel() * b_host.element_size()
+        e2e = {"value": world * NRHS / tmax, "unit": "solves/s", "h2d_bytes_per_step": int(nbytes),
+               "d2h_bytes_per_step": int(nbytes)}
+
+    # ---- CPU baseline (rank 0, N=1): C restatement of the reference's FP64 CG
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(U.cpu().numpy(), b[NRHS - 1].cpu().numpy(), int(np.mean(it64)), args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": t_max * 1e3,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 arithmetic on f16 storage + f64 reliable updates",
+            "data": "synthetic (seeded links exp(i*0.2*H), point + Gaussian sources)",
+            "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, SHAPE)), "kappa": KAPPA,
+                       "nrhs": NRHS, "tol": TOL, "parallelism": f"replicas x{world} (independent solves)",
+                       "l2": "working set > 126 MB L2 (no flush needed)"},
+            "fp64_cg": {"solves_per_s": fp64_sps * world, "iters": it64, "note": "plain FP64 CG, one RHS at a time"},
+            "speedup_vs_fp64": value / (fp64_sps * world),
+            "solve": {"iters_min": min(iters), "iters_max": max(iters), "max_true_res": res, "all_converged": conv,
+                      "reliable_updates_max": max(s["reliable_updates"] for s in all_stats[-1])},
+            "roofline": {"bound": "hbm", "kernel": "hop (FP16 storage, 12-real links, 16 RHS, EO parity)",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": hop_bytes,
+                         "ms_per_launch": hop_ms, "traffic": traffic},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------- CPU legs
+def cpu_baseline(U4, b_full, iters_to_converge: int, seconds: float):
+    """Time FP64 EO CG iterations of the C restatement on all host cores on
+    the full 24^3x48 system for ~`seconds`, and convert to solves/s with the
+    iteration count FP64 CG needs on this system."""
+    from oracle import cpu as C
+    from oracle import wilson as W
+
+    C.build()
+    cw = C.CpuWilson(U4, SHAPE, BC, MASS)
+    be = W.pack(b_full[None], 0)[0]
+    x, k, _ = cw.cg(be, 0.0, 1)  # warm-up (1 iteration)
+    n = 2
+    t0 = time.perf_counter()
+    x, k, _ = cw.cg(be, 0.0, n)
+    t1 = time.perf_counter()
+    per = (t1 - t0) / n
+    n2 = max(1, int(seconds / max(per, 1e-6)) - n)
+    if n2 > 0:
+        t2 = time.perf_counter()
+        cw.cg(be, 0.0, n2)
+        per = (time.perf_counter() - t2) / n2
+        n += n2
+    return {"value": 1.0 / (per * iters_to_converge), "unit": "solves/s", "cores": C.threads(), "kind": "port",
+            "sample": f"{n} FP64 CG iterations of M^dag M on the full 24^3x48 system, 1 RHS; solves/s = 1/"
+                      f"(s/iter x {iters_to_converge} iters to 1e-10)", "s_per_iter": per}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    # The reference (JAX) is not installable offline here; its CPU path is timed
+    # through the C restatement of its even-odd CG (oracle/c) on all host cores.
+    import torch
+
+    from oracle import cpu as C
+    from oracle import wilson as W
+
+    U, eta = make_inputs(torch, torch.device("cpu"), seed=0)
+    C.build()
+    cw = C.CpuWilson(U.numpy(), SHAPE, BC, MASS)
+    be = cw.normal(W.pack(eta[12:13].numpy(), 0)[0])  # an even RHS of the system; only timing is used
+    per_step = []
+    its = 4
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        cw.cg(be, 0.0, its)
+        dt = (time.perf_counter() - t0) / its
+        if i >= args.warmup:
+            per_step.append(dt)
+    per = float(np.mean(per_step))
+    iters = args.ref_iters
+    value = 1.0 / (per * iters)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * its * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, SHAPE)), "kappa": KAPPA},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": C.threads(), "kind": "port",
+                             "sample": f"{its} FP64 CG iterations per step on the full system, 1 RHS; solves/s = "
+                                       f"1/(s/iter x {iters} iterations FP64 CG needs to 1e-10)"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "jaxQFT needs JAX, which is not installable offline; its EO CG is timed via the C restatement"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--fp64-all", action="store_true", help="time plain FP64 CG on all 16 RHS (default 4)")
+    ap.add_argument("--ref-iters", type=int, default=178,
+                    help="FP64 CG iterations to 1e-10 on this system (measured by the GPU FP64 solve)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

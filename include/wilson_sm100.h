@@ -158,6 +158,24 @@ wl_status wl_engine_poll(wl_engine* eng, int* status, int* n_active);
 wl_status wl_engine_retire(wl_engine* eng, int slot, void* x, wl_solve_stats* stats);
 /* Size in bytes of the engine's device allocations (for HBM admission). */
 int64_t wl_engine_bytes(const wl_ctx* ctx, int op, int inner_prec, int nslots);
+/* The cudaStream_t the engine runs on (for events / stream ordering). */
+void* wl_engine_stream(wl_engine* eng);
+
+/* Instrumentation (no counterpart in the reference) ----------------------- */
+/* Time `reps` launches of the engine's dominant kernel (the iterated-precision
+   hop over all slots, as the CG runs it) with CUDA events on the engine stream.
+   Writes the mean milliseconds per launch and the algorithmic HBM bytes one
+   launch must move (every link and spinor touched once). Synchronous. */
+wl_status wl_engine_time_hop(wl_engine* eng, int reps, double* ms_per_launch, double* bytes_per_launch);
+/* Apply the engine's iterated (sloppy-precision) operator to one
+   reference-layout field through slot 0's buffers, for testing the FP16/FP32
+   operators against FP64: stage 0 -> K_oe x_e (odd sites of out), 1 -> M x_e,
+   2 -> M^dag M x_e (EO engines; even sites of out), 3 -> D x, 4 -> D^dag D x
+   (full-lattice engines).  Overwrites slot 0's work fields.  Synchronous. */
+wl_status wl_engine_debug_apply(wl_engine* eng, int stage, double mass, const void* in, void* out);
+/* Number of kernels this library has launched in the process so far
+   (graph launches count every kernel node of the graph). */
+int64_t wl_kernel_launches(void);
 
 /* Pseudofermion force ----------------------------------------------------- */
 /* F = pseudofermion_force_from_solution(U, X, Y) (su3_wilson_nf2.py:1556-1576):

@@ -47,6 +47,8 @@ static std::atomic<unsigned long long> g_gauge_ids{1};
 extern "C" void wl_release_solve_cache(wl_ctx* ctx);
 
 static thread_local std::string g_static_err;
+static std::atomic<long long> g_launches{0};
+extern "C" int64_t wl_kernel_launches(void) { return g_launches.load(); }
 
 static inline void set_err(wl_ctx* ctx, const std::string& m);
 #define WL_FAIL(ctx, code, msg) \
@@ -169,6 +171,7 @@ static dim3 grid_for(const Geom& g, const Tune& t, int nrhs, int npar) {
 template <bool DAG, class IDX, class LF, class SF, class EPI>
 static void launch_hop(const Tune& t, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st) {
   dim3 grid = grid_for(a.g, t, a.nrhs, npar), block(t.bx, t.by, 1);
+  g_launches++;
   switch (t.nr) {
     case 4: hop_kernel<DAG, 4, IDX><<<grid, block, 0, st>>>(a); break;
     case 2: hop_kernel<DAG, 2, IDX><<<grid, block, 0, st>>>(a); break;
@@ -187,6 +190,7 @@ static void launch_site(const Tune& t, const Geom& g, int parity0, int npar, int
   a.f = f;
   a.red = red;
   dim3 grid = grid_for(g, t, nrhs, npar), block(t.bx, t.by, 1);
+  g_launches++;
   switch (t.nr) {
     case 4: site_kernel<4><<<grid, block, 0, st>>>(a); break;
     case 2: site_kernel<2><<<grid, block, 0, st>>>(a); break;
@@ -282,6 +286,7 @@ static wl_status gauge_fill(wl_gauge* G, const void* U) {
   WL_CUDA(ctx, cudaMemsetAsync(G->uerr, 0, sizeof(unsigned int), ctx->stream));
   GaugeOut o{G->d18, G->d12, G->s12, G->h12, G->uerr};
   dim3 grid((g.Vh + 127) / 128, 2, 4);
+  g_launches++;
   gauge_convert_kernel<<<grid, 128, 0, ctx->stream>>>(g, G->ref_copy, o);
   return check_launch(ctx, "gauge_convert_kernel");
 }
@@ -489,6 +494,7 @@ extern "C" wl_status wl_pf_force(wl_ctx* ctx, wl_gauge* G, const void* X, const 
   A.coef = coef;
   A.accumulate = accumulate;
   dim3 grid((g.Vh + 127) / 128, 2, 4);
+  g_launches++;
   pf_force_kernel<<<grid, 128, 0, ctx->stream>>>(A);
   return check_launch(ctx, "pf_force_kernel");
 }
@@ -534,7 +540,19 @@ struct wl_engine {
   // graph
   cudaGraphExec_t gexec = nullptr;
   bool graph_built = false;
+  long long graph_kernels = 0;  // kernel nodes per captured iteration
 };
+
+struct EngineStream {
+  cudaStream_t st;
+};
+static std::map<const wl_engine*, cudaStream_t> g_engine_streams;
+static std::mutex g_es_mu;
+
+static cudaStream_t engine_stream(const wl_engine* E) {
+  std::lock_guard<std::mutex> lk(g_es_mu);
+  return g_engine_streams[E];
+}
 
 static const int kEngineDoubles = 12;
 static const int kEngineInts = 8;
@@ -548,6 +566,14 @@ int64_t engine_bytes_impl(const Geom& g, int op, int sprec, int n) {
   b += (int64_t)field_bytes(sprec, g.Vh, n, 1);                          // t1
   b += (int64_t)n * (g.Vh / 32 + 1) * 2 * sizeof(double) + 4096;
   return b;
+}
+
+static int64_t hop_bytes(const Geom& g, int sprec, int nrhs) {
+  // one EO hop: 8 links per target site (4 fwd own parity + 4 bwd other) and,
+  // per RHS, one source spinor and one output spinor per site.
+  const double L = sprec == P_DOUBLE ? 144.0 : (sprec == P_SINGLE ? 48.0 : 24.0);
+  const double S = sprec == P_DOUBLE ? 192.0 : (sprec == P_SINGLE ? 96.0 : 52.0);
+  return (int64_t)((double)g.Vh * (8.0 * L + nrhs * 2.0 * S));
 }
 
 extern "C" int64_t wl_engine_bytes(const wl_ctx* ctx, int op, int inner_prec, int nslots) {
@@ -644,6 +670,33 @@ template <> struct SloppyLinks<P_HALF> {
   using type = LinkField<L_H12>;
   static type get(wl_gauge* G) { return type{G->h12, G->ctx->g.Vh}; }
 };
+
+template <int S>
+static void time_hop_impl(wl_engine* E, cudaStream_t st, int reps, float* ms) {
+  using SFS = SpinorField<S>;
+  using LS = typename SloppyLinks<S>::type;
+  HopArgs<LS, SFS, EpiXpay<SFS, false>> A{};
+  A.g = E->ctx->g;
+  A.links = SloppyLinks<S>::get(E->gauge);
+  sf2<S>(E->p, A.src);
+  A.parity0 = 1;
+  A.nrhs = E->n;
+  A.mask = nullptr;
+  sf2<S>(E->t1, A.epi.out);
+  A.epi.has_self = 0;
+  A.epi.b = E->neg_half;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  launch_hop<false, IdxCompact>(E->ts, A, 1, st);
+  cudaEventRecord(e0, st);
+  for (int i = 0; i < reps; ++i) launch_hop<false, IdxCompact>(E->ts, A, 1, st);
+  cudaEventRecord(e1, st);
+  cudaEventSynchronize(e1);
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+}
 
 // Enqueue the FP64 normal operator on x64 ending in the true residual
 // rs = convert(b - A x64), r2_true = |b - A x64|^2, for the slots in `mask`.
@@ -758,6 +811,7 @@ static void enqueue_iteration(wl_engine* E, cudaStream_t st) {
     }
   }
   CGScalars Sc = scalars_of(E);
+  g_launches++;
   cg_decide_kernel<<<1, 128, 0, st>>>(Sc, n);
   {  // x64 += xs ; xs = 0  (reliable-update slots)
     FAccumX<SFS> f;
@@ -766,6 +820,7 @@ static void enqueue_iteration(wl_engine* E, cudaStream_t st) {
     launch_site(E->tsite, g, 0, E->npar, n, E->ru, f, Reduce{}, st);
   }
   enqueue_true_residual<S>(E, E->ru, st);
+  g_launches++;
   cg_finalize_kernel<<<1, 128, 0, st>>>(Sc, n);
   {  // p = rs + beta p
     FUpdateP<SFS> f;
@@ -819,7 +874,123 @@ static void enqueue_admit(wl_engine* E, const void* b, int use_x0, const void* x
     sf2<S>(E->xs, z.out);
     launch_site(E->tsite, g, par0, E->npar, n, adm, z, Reduce{}, st);
   }
+  g_launches++;
   admit_state_kernel<<<1, 128, 0, st>>>(scalars_of(E), adm, use_x0, n);
+}
+
+// Debug/test path: apply the sloppy operator to one field via slot 0.
+template <int S>
+static void debug_apply_impl(wl_engine* E, int stage, double mass, const void* in, void* out, cudaStream_t st) {
+  using SFS = SpinorField<S>;
+  using SFD = SpinorField<P_DOUBLE>;
+  using LS = typename SloppyLinks<S>::type;
+  const Geom& g = E->ctx->g;
+  LS L = SloppyLinks<S>::get(E->gauge);
+  const double m0 = mass + 4.0;
+  std::vector<double> coef = {1.0, -0.5, 0.5 / (m0 * m0), m0};
+  double* dc = E->r2_true;  // scratch: 4 doubles (engine has >= 1 slot; r2_true has n entries)
+  double* tmp;
+  cudaMalloc(&tmp, 4 * sizeof(double));
+  cudaMemcpyAsync(tmp, coef.data(), 4 * sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaStreamSynchronize(st);
+  (void)dc;
+  const double *one = tmp, *nh = tmp + 1, *ha = tmp + 2, *mm = tmp + 3;
+  const int npar = E->npar;
+  const int par0 = 0;
+  // in -> b64 (slot 0) -> p (sloppy)
+  {
+    FPack<SFD> f;
+    f.g = g;
+    f.in = sref(in, g);
+    f.rhs_off = 0;
+    sf2<P_DOUBLE>(E->b64, f.out);
+    launch_site(E->tsite, g, par0, npar, 1, nullptr, f, red_to(E, E->r2_true), st);
+    FConvert<SFD, SFS> cv;
+    sf2<P_DOUBLE>(E->b64, cv.in);
+    sf2<S>(E->p, cv.out);
+    launch_site(E->tsite, g, par0, npar, 1, nullptr, cv, red_to(E, E->r2_true), st);
+  }
+  IField* res = &E->y;
+  int res_par = 0, res_np = npar;
+  if (E->prm.op == WL_SOLVE_EO_NORMAL) {
+    HopArgs<LS, SFS, EpiXpay<SFS, false>> A{};
+    A.g = g; A.links = L; A.nrhs = 1;
+    sf2<S>(E->p, A.src); A.parity0 = 1; sf2<S>(E->t1, A.epi.out); A.epi.b = nh;
+    launch_hop<false, IdxCompact>(E->ts, A, 1, st);
+    if (stage == 0) {
+      res = &E->t1;
+      res_par = 1;
+      res_np = 1;
+    } else {
+      HopArgs<LS, SFS, EpiXpay<SFS, false>> B{};
+      B.g = g; B.links = L; B.nrhs = 1;
+      sf2<S>(E->t1, B.src); B.parity0 = 0; sf2<S>(E->y, B.epi.out); sf2<S>(E->p, B.epi.self);
+      B.epi.has_self = 1; B.epi.a = one; B.epi.b = ha;
+      launch_hop<false, IdxCompact>(E->ts, B, 1, st);
+      if (stage >= 2) {
+        HopArgs<LS, SFS, EpiXpay<SFS, false>> C{};
+        C.g = g; C.links = L; C.nrhs = 1;
+        sf2<S>(E->y, C.src); C.parity0 = 1; sf2<S>(E->t1, C.epi.out); C.epi.b = nh;
+        launch_hop<true, IdxCompact>(E->ts, C, 1, st);
+        HopArgs<LS, SFS, EpiXpay<SFS, false>> D{};
+        D.g = g; D.links = L; D.nrhs = 1;
+        sf2<S>(E->t1, D.src); D.parity0 = 0; sf2<S>(E->xs, D.epi.out); sf2<S>(E->y, D.epi.self);
+        D.epi.has_self = 1; D.epi.a = one; D.epi.b = ha;
+        launch_hop<true, IdxCompact>(E->ts, D, 1, st);
+        res = &E->xs;
+      }
+    }
+  } else {
+    HopArgs<LS, SFS, EpiXpay<SFS, false>> A{};
+    A.g = g; A.links = L; A.nrhs = 1;
+    sf2<S>(E->p, A.src); A.parity0 = 0; sf2<S>(E->y, A.epi.out); sf2<S>(E->p, A.epi.self);
+    A.epi.has_self = 1; A.epi.a = mm; A.epi.b = nh;
+    launch_hop<false, IdxCompact>(E->ts, A, 2, st);
+    if (stage >= 4) {
+      HopArgs<LS, SFS, EpiXpay<SFS, false>> B{};
+      B.g = g; B.links = L; B.nrhs = 1;
+      sf2<S>(E->y, B.src); B.parity0 = 0; sf2<S>(E->xs, B.epi.out); sf2<S>(E->y, B.epi.self);
+      B.epi.has_self = 1; B.epi.a = mm; B.epi.b = nh;
+      launch_hop<true, IdxCompact>(E->ts, B, 2, st);
+      res = &E->xs;
+    }
+  }
+  // result (sloppy) -> FP64 (x64 slot 0, or t64 for odd) -> reference layout
+  IField dst = res_np == 1 && res_par == 1 ? E->t64 : E->x64;
+  {
+    IField srcv = *res;
+    FConvert<SFS, SFD> cv;
+    sf2<S>(srcv, cv.in);
+    sf2<P_DOUBLE>(dst, cv.out);
+    launch_site(E->tsite, g, res_np == 1 ? res_par : 0, res_np, 1, nullptr, cv, red_to(E, E->r2_true), st);
+  }
+  cudaMemsetAsync(out, 0, (size_t)g.V * 12 * sizeof(double2), st);
+  {
+    FUnpack f;
+    f.g = g;
+    sf2<P_DOUBLE>(dst, f.in);
+    f.out = sref(out, g);
+    f.rhs_off = 0;
+    launch_site(E->tsite, g, res_np == 1 ? res_par : 0, res_np, 1, nullptr, f, Reduce{}, st);
+  }
+  cudaStreamSynchronize(st);
+  cudaFree(tmp);
+}
+
+extern "C" wl_status wl_engine_debug_apply(wl_engine* E, int stage, double mass, const void* in, void* out) {
+  if (!E || !in || !out) WL_FAIL(nullptr, WL_ERR_ARG, "null argument");
+  wl_ctx* ctx = E->ctx;
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  const bool eo = E->prm.op == WL_SOLVE_EO_NORMAL;
+  if ((eo && (stage < 0 || stage > 2)) || (!eo && stage != 3 && stage != 4))
+    WL_FAIL(ctx, WL_ERR_ARG, "stage does not match the engine's operator");
+  cudaStream_t st = engine_stream(E);
+  switch (E->sprec) {
+    case P_HALF: debug_apply_impl<P_HALF>(E, stage, mass, in, out, st); break;
+    case P_SINGLE: debug_apply_impl<P_SINGLE>(E, stage, mass, in, out, st); break;
+    default: debug_apply_impl<P_DOUBLE>(E, stage, mass, in, out, st); break;
+  }
+  return check_launch(ctx, "wl_engine_debug_apply");
 }
 
 static void enqueue_iteration_any(wl_engine* E, cudaStream_t st) {
@@ -905,23 +1076,16 @@ static Tune pick_tune(wl_engine* E, cudaStream_t st) {
     t.bx = 128;
     t.by = std::max(1, std::min(4, (E->n + t.nr - 1) / t.nr));
   }
+  const char* verb = std::getenv("WL_VERBOSE");
+  if (verb && verb[0] == '1')
+    std::fprintf(stderr, "[wl] tune vh=%d prec=%d nslots=%d op=%d -> nr=%d bx=%d by=%d\n", k.vh, k.prec, k.nslots,
+                 k.op, t.nr, t.bx, t.by);
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune_cache[k] = t;
   return t;
 }
 
 // ------------------------------------------------------------------ engine API
-struct EngineStream {
-  cudaStream_t st;
-};
-static std::map<const wl_engine*, cudaStream_t> g_engine_streams;
-static std::mutex g_es_mu;
-
-static cudaStream_t engine_stream(const wl_engine* E) {
-  std::lock_guard<std::mutex> lk(g_es_mu);
-  return g_engine_streams[E];
-}
-
 extern "C" void wl_engine_destroy(wl_engine* E) {
   if (!E) return;
   cudaSetDevice(E->ctx->device);
@@ -1098,7 +1262,10 @@ static wl_status build_graph(wl_engine* E, cudaStream_t st) {
   wl_ctx* ctx = E->ctx;
   cudaGraph_t graph;
   WL_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  const long long before = g_launches.load();
   enqueue_iteration_any(E, st);
+  E->graph_kernels = g_launches.load() - before;
+  g_launches -= E->graph_kernels;  // captured, not launched
   cudaError_t e = cudaStreamEndCapture(st, &graph);
   if (e != cudaSuccess) {
     ctx->err = std::string("graph capture: ") + cudaGetErrorString(e);
@@ -1131,10 +1298,34 @@ extern "C" wl_status wl_engine_step(wl_engine* E, int iters) {
     if (s != WL_OK) return s;
   }
   for (int i = 0; i < iters; ++i) {
-    if (E->prm.use_graph) WL_CUDA(ctx, cudaGraphLaunch(E->gexec, st));
-    else enqueue_iteration_any(E, st);
+    if (E->prm.use_graph) {
+      WL_CUDA(ctx, cudaGraphLaunch(E->gexec, st));
+      g_launches += E->graph_kernels;
+    } else {
+      enqueue_iteration_any(E, st);
+    }
   }
   return check_launch(ctx, "wl_engine_step");
+}
+
+extern "C" void* wl_engine_stream(wl_engine* E) { return E ? (void*)engine_stream(E) : nullptr; }
+
+extern "C" wl_status wl_engine_time_hop(wl_engine* E, int reps, double* ms, double* bytes) {
+  if (!E || !ms || !bytes || reps <= 0) WL_FAIL(nullptr, WL_ERR_ARG, "bad argument");
+  wl_ctx* ctx = E->ctx;
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = engine_stream(E);
+  float t = 0.f;
+  switch (E->sprec) {
+    case P_HALF: time_hop_impl<P_HALF>(E, st, reps, &t); break;
+    case P_SINGLE: time_hop_impl<P_SINGLE>(E, st, reps, &t); break;
+    default: time_hop_impl<P_DOUBLE>(E, st, reps, &t); break;
+  }
+  wl_status s = check_launch(ctx, "wl_engine_time_hop");
+  if (s != WL_OK) return s;
+  *ms = (double)t / reps;
+  *bytes = (double)hop_bytes(ctx->g, E->sprec, E->n);
+  return WL_OK;
 }
 
 extern "C" wl_status wl_engine_poll(wl_engine* E, int* status, int* n_active) {

@@ -223,8 +223,13 @@ template <> struct SpinorField<P_HALF> {
     for (int a = 0; a < 4; ++a)
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) mx = fmaxf(mx, fmaxf(fabsf(s.v[a][cc].re), fabsf(s.v[a][cc].im)));
-    float inv = mx > 0.f ? 1.0f / mx : 0.f;
-    norm[(long long)rhs * vh + c] = mx;
+    // A site whose largest component is below FLT_MIN is stored as zero: 1/mx
+    // would overflow to Inf there and turn exact zeros into NaN (0 * Inf).
+    // Such sites occur far from a point source, where Krylov vectors decay
+    // over tens of lattice spacings.
+    const bool keep = mx >= 1.17549435e-38f;
+    const float inv = keep ? 1.0f / mx : 0.f;
+    norm[(long long)rhs * vh + c] = keep ? mx : 0.f;
     uint4* b = ptr + rhs * rstride + c;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {

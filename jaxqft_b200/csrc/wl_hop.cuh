@@ -207,6 +207,7 @@ WL_D void reduce_rhs(const double (&val)[NR], const Reduce& R, int nrhs, const i
   __threadfence();
   __syncthreads();
   if (tid == 0) {
+    __threadfence();
     unsigned t = atomicAdd(&R.counter[blockIdx.y], 1u);
     s_last = (t == (unsigned)nblk - 1);
   }

@@ -38,6 +38,7 @@ EXPORTS = (
     "wl_ctx_synchronize", "wl_eo_maps", "wl_gauge_create", "wl_gauge_update", "wl_gauge_unitarity",
     "wl_gauge_destroy", "wl_apply", "wl_solve", "wl_engine_create", "wl_engine_destroy", "wl_engine_admit",
     "wl_engine_step", "wl_engine_poll", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
+    "wl_engine_stream", "wl_engine_time_hop", "wl_kernel_launches", "wl_engine_debug_apply",
 )
 
 
@@ -99,6 +100,10 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wl_engine_retire": (i, [vp, i, vp, ctypes.POINTER(WLSolveStats)]),
         "wl_engine_bytes": (ctypes.c_int64, [vp, i, i, i]),
         "wl_pf_force": (i, [vp, vp, vp, vp, d, i, vp]),
+        "wl_engine_stream": (vp, [vp]),
+        "wl_engine_time_hop": (i, [vp, i, pd, pd]),
+        "wl_kernel_launches": (ctypes.c_int64, []),
+        "wl_engine_debug_apply": (i, [vp, i, d, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -112,6 +117,11 @@ class WilsonError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
         self.code = code
+
+
+def kernel_launches() -> int:
+    """Kernels launched by libwilson_sm100 in this process so far."""
+    return int(load_library().wl_kernel_launches())
 
 
 def _require_cuda():
@@ -349,6 +359,29 @@ class Engine:
         s = WLSolveStats()
         self.ctx._check(self.ctx.lib.wl_engine_retire(self.handle, int(slot), _ptr(out), ctypes.byref(s)))
         return out, dict(iters=s.iters, reliable_updates=s.reliable_updates, status=s.status, true_res=s.true_res)
+
+    @property
+    def stream(self):
+        """The engine's CUDA stream as a torch ExternalStream."""
+        import torch
+
+        return torch.cuda.ExternalStream(int(self.ctx.lib.wl_engine_stream(self.handle)), device=self.ctx.device)
+
+    def debug_apply(self, stage: int, mass: float, x):
+        """The engine's iterated-precision operator applied to one field (see
+        wl_engine_debug_apply): 0 K_oe, 1 M, 2 M^dag M (EO); 3 D, 4 D^dag D (full)."""
+        import torch
+
+        x = _c128(x, self.ctx.device)
+        out = torch.empty_like(x)
+        self.ctx._check(self.ctx.lib.wl_engine_debug_apply(self.handle, int(stage), float(mass), _ptr(x), _ptr(out)))
+        return out
+
+    def time_hop(self, reps: int = 20):
+        """(ms per launch, algorithmic bytes per launch) of the iterated hop kernel."""
+        ms, by = ctypes.c_double(), ctypes.c_double()
+        self.ctx._check(self.ctx.lib.wl_engine_time_hop(self.handle, int(reps), ctypes.byref(ms), ctypes.byref(by)))
+        return float(ms.value), float(by.value)
 
     def close(self):
         if getattr(self, "handle", None) is not None and self.handle.value:

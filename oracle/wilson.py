@@ -421,6 +421,16 @@ def hot_links(rng, shape, batch, scale):
     return expm_su3(ta(a))
 
 
+def hot_links_eigh(rng, shape, batch, scale):
+    """Same distribution as ``hot_links`` with exp(X) = V exp(-i lam) V^dag from
+    the eigendecomposition of the Hermitian iX (fast at full lattice volumes)."""
+    lshape = (batch, ND, *shape, 3, 3)
+    a = scale * (rng.standard_normal(lshape) + 1j * rng.standard_normal(lshape))
+    X = ta(a)
+    lam, V = np.linalg.eigh(1j * X)
+    return np.einsum("...ij,...j,...kj->...ik", V, np.exp(-1j * lam), np.conj(V), optimize=True)
+
+
 def gaussian_spinor(rng, shape, batch):
     fshape = (batch, *shape, 4, 3)
     return (rng.standard_normal(fshape) + 1j * rng.standard_normal(fshape)) / np.sqrt(2.0)

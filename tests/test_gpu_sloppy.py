@@ -1,0 +1,121 @@
+"""The FP16 and FP32 iterated operators of the solver engine against the FP64
+oracle, on Gaussian and on point-source fields (the latter have most sites
+exactly zero, the hard case for per-site FP16 norms).
+
+Tolerances (relative, Frobenius): FP64 1e-13; FP32 storage + 12-real links
+2e-6; FP16 storage (per-site norm) + 12-real FP16 links with FP32 arithmetic
+4e-3 per application of M^dag M.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import wilson as W
+from tests.conftest import load_golden, rel
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("CUDA device required", allow_module_level=True)
+
+from jaxqft_b200.lib import Engine, WilsonContext  # noqa: E402
+
+TOLS = {"double": 1e-13, "single": 2e-6, "half": 4e-3}
+
+
+def _fields(shape, seed):
+    rng = np.random.default_rng(seed)
+    gauss = W.gaussian_spinor(rng, shape, 1)[0]
+    point = np.zeros_like(gauss)
+    point[0, 0, 0, 0, 1, 2] = 1.0
+    return {"gauss": gauss, "point": point}
+
+
+@pytest.fixture(scope="module")
+def setup():
+    shape = (4, 4, 4, 8)
+    rng = np.random.default_rng(7)
+    U = W.hot_links(rng, shape, 1, 0.2)
+    bc = (1, 1, 1, -1)
+    ctx = WilsonContext(shape, bc=bc)
+    gauge = ctx.gauge(torch.from_numpy(U[0]))
+    return shape, U, bc, ctx, gauge
+
+
+@pytest.mark.parametrize("inner", ["double", "single", "half"])
+@pytest.mark.parametrize("src", ["gauss", "point"])
+def test_eo_sloppy_operators(setup, inner, src):
+    shape, U, bc, ctx, gauge = setup
+    m = -0.2962963
+    eng = Engine(ctx, gauge, 1, op="eo_normal", inner=inner)
+    xe = W.project(_fields(shape, 1)[src][None], 0)
+    refs = {
+        0: W.K_block(U, xe, bc, 0),
+        1: W.schur_even(U, xe, m, bc, normalized=True),
+    }
+    refs[2] = W.schur_even(U, refs[1], m, bc, normalized=True, dag=True)
+    for stage, ref in refs.items():
+        out = eng.debug_apply(stage, m, torch.from_numpy(xe[0])).cpu().numpy()
+        assert rel(out, ref[0]) < TOLS[inner], (inner, src, stage, rel(out, ref[0]))
+    eng.close()
+
+
+@pytest.mark.parametrize("inner", ["double", "single", "half"])
+def test_full_sloppy_operators(setup, inner):
+    shape, U, bc, ctx, gauge = setup
+    m = 0.1
+    eng = Engine(ctx, gauge, 1, op="normal", inner=inner)
+    for src, x in _fields(shape, 2).items():
+        out = eng.debug_apply(3, m, torch.from_numpy(x)).cpu().numpy()
+        assert rel(out, W.apply_D(U, x[None], m, bc)[0]) < TOLS[inner], (inner, src)
+        out = eng.debug_apply(4, m, torch.from_numpy(x)).cpu().numpy()
+        assert rel(out, W.apply_normal(U, x[None], m, bc)[0]) < TOLS[inner], (inner, src)
+    eng.close()
+
+
+@pytest.mark.parametrize("inner", ["single", "half"])
+@pytest.mark.parametrize("op", ["eo_normal", "normal"])
+def test_point_source_solves_converge(setup, inner, op):
+    shape, U, bc, ctx, gauge = setup
+    m = -0.2962963
+    eta = np.zeros((12, *shape, 4, 3), dtype=np.complex128)
+    for k in range(12):
+        eta[k, 0, 0, 0, 0, k // 3, k % 3] = 1.0
+    if op == "eo_normal":
+        b = ctx.apply("SCHUR_E_DAG", gauge, m, torch.from_numpy(eta), normalized=True)
+    else:
+        b = ctx.apply("DDAG", gauge, m, torch.from_numpy(eta))
+    x, st = ctx.solve(gauge, b, m, op=op, tol=1e-10, maxiter=3000, inner=inner)
+    assert all(s["status"] == 2 for s in st), st
+    bn, xn = b.cpu().numpy(), x.cpu().numpy()
+    for r in range(12):
+        if op == "eo_normal":
+            s = W.schur_even(U, xn[r][None], m, bc, normalized=True)
+            Ax = W.schur_even(U, s, m, bc, normalized=True, dag=True)[0]
+        else:
+            Ax = W.apply_normal(U, xn[r][None], m, bc)[0]
+        assert np.linalg.norm(bn[r] - Ax) / np.linalg.norm(bn[r]) <= 1e-10
+
+
+def test_point_source_long_lattice_half():
+    """Regression: on a long lattice a point-source Krylov vector decays below
+    FLT_MIN far from the source; the FP16 per-site scale must then store zeros
+    (1/max would overflow and turn exact zeros into NaN)."""
+    shape = (4, 4, 4, 128)
+    rng = np.random.default_rng(9)
+    U = W.hot_links(rng, shape, 1, 0.2)
+    bc = (1, 1, 1, -1)
+    m = -0.2962963
+    ctx = WilsonContext(shape, bc=bc)
+    gauge = ctx.gauge(torch.from_numpy(U[0]))
+    eta = np.zeros((2, *shape, 4, 3), dtype=np.complex128)
+    eta[0, 0, 0, 0, 0, 0, 0] = 1.0
+    eta[1, 0, 0, 0, 0, 3, 2] = 1.0
+    b = ctx.apply("SCHUR_E_DAG", gauge, m, torch.from_numpy(eta), normalized=True)
+    x, st = ctx.solve(gauge, b, m, op="eo_normal", tol=1e-10, maxiter=3000, inner="half")
+    assert all(s["status"] == 2 for s in st), st
+    bn, xn = b.cpu().numpy(), x.cpu().numpy()
+    for r in range(2):
+        s = W.schur_even(U, xn[r][None], m, bc, normalized=True)
+        Ax = W.schur_even(U, s, m, bc, normalized=True, dag=True)[0]
+        assert np.linalg.norm(bn[r] - Ax) / np.linalg.norm(bn[r]) <= 1e-10
