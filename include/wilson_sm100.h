@@ -177,6 +177,21 @@ wl_status wl_engine_debug_apply(wl_engine* eng, int stage, double mass, const vo
    (graph launches count every kernel node of the graph). */
 int64_t wl_kernel_launches(void);
 
+/* Allocation-free operator (no counterpart in the reference) -------------- */
+/* out = S_e^dag S_e in, exactly what wl_apply(WL_OP_SCHUR_E_NORMAL) computes,
+   for callers that cannot call cudaMalloc: a JAX/XLA custom-call handler
+   works in device memory the framework already owns (JAX preallocates most
+   of the GPU), and latency-critical loops avoid the allocator's implicit
+   synchronisation.  The two intermediate fields live in a 64 MiB static
+   device array that every GPU loading this library holds until exit, so
+   2 * nrhs * volume * 192 bytes must fit (nrhs * volume <= 174762, e.g. one
+   16^3x32 field); larger requests return WL_ERR_ARG.  The first call on a
+   device resolves the array's address with that device current; make it
+   before any stream capture.  All calls share the array: calls that overlap
+   on the GPU (different streams or contexts of one device) race. */
+wl_status wl_apply_schur_normal_noalloc(wl_ctx* ctx, wl_gauge* gauge, double mass, unsigned flags,
+                                        const void* in, void* out, int nrhs);
+
 /* Pseudofermion force ----------------------------------------------------- */
 /* F = pseudofermion_force_from_solution(U, X, Y) (su3_wilson_nf2.py:1556-1576):
    F[mu][x] = TA( (c1 - c2)^T ), link-shaped complex128 BMXYIJ.  If

@@ -1498,3 +1498,67 @@ extern "C" void wl_release_solve_cache(wl_ctx* ctx) {
     }
   }
 }
+
+// ============================================================== allocation-free Schur normal operator
+// Some callers cannot call cudaMalloc: a JAX/XLA custom-call handler runs with
+// device memory owned by the framework (JAX preallocates most of the GPU at
+// start-up, so an allocation made from inside the handler can fail), and
+// latency-critical serving loops avoid the allocator's implicit device
+// synchronisation.  wl_apply(WL_OP_SCHUR_E_NORMAL) allocates its two
+// intermediate fields on first use; this variant takes them from a fixed
+// file-scope device array instead and allocates nothing.
+static constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;  // 64 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array for ctx->device.  Resolved once per
+// device (with that device current) and cached; host code must never use the
+// symbol itself as a device pointer.
+static wl_status noalloc_scratch(wl_ctx* ctx, void** out) {
+  if (ctx->device < 0 || ctx->device >= 64) WL_FAIL(ctx, WL_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[ctx->device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      ctx->err = std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e);
+      return WL_ERR_CUDA;
+    }
+    g_noalloc_ptr[ctx->device] = p;
+  }
+  *out = g_noalloc_ptr[ctx->device];
+  return WL_OK;
+}
+
+extern "C" wl_status wl_apply_schur_normal_noalloc(wl_ctx* ctx, wl_gauge* G, double mass, unsigned flags,
+                                                   const void* in, void* out, int nrhs) {
+  if (!ctx || !G || !in || !out) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
+  if (in == out) WL_FAIL(ctx, WL_ERR_ARG, "in and out must not alias");
+  if (nrhs <= 0) WL_FAIL(ctx, WL_ERR_ARG, "nrhs must be positive");
+  const Geom& g = ctx->g;
+  const size_t fbytes = (size_t)nrhs * g.V * 12 * sizeof(double2);
+  if (2 * fbytes > kNoAllocScratchBytes)
+    WL_FAIL(ctx, WL_ERR_ARG,
+            "wl_apply_schur_normal_noalloc needs " + std::to_string(2 * fbytes) +
+                " bytes of scratch (2 * nrhs * volume * 192) but its static scratch holds " +
+                std::to_string(kNoAllocScratchBytes) + " bytes (nrhs * volume <= 174762)");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  void* scratch = nullptr;
+  wl_status s = noalloc_scratch(ctx, &scratch);
+  if (s != WL_OK) return s;
+  // t1 holds K_oe x on odd sites, y holds M x on even sites; each kernel reads
+  // only the sites the previous one wrote, so neither needs clearing.
+  void* t1 = scratch;
+  void* y = static_cast<char*>(scratch) + fbytes;
+  const bool norm = (flags & WL_FLAG_NORMALIZED) != 0;
+  const double m0 = mass + 4.0;
+  const double c0 = norm ? 1.0 : m0;
+  const double c1 = norm ? 0.5 / (m0 * m0) : 0.5 / m0;
+  WL_CUDA(ctx, cudaMemsetAsync(out, 0, fbytes, ctx->stream));  // odd sites of the result are zero
+  ref_hop<false>(ctx, G, in, t1, nullptr, 0.0, -0.5, nrhs, 1, 1);
+  ref_hop<false>(ctx, G, t1, y, in, c0, c1, nrhs, 0, 1);
+  ref_hop<true>(ctx, G, y, t1, nullptr, 0.0, -0.5, nrhs, 1, 1);
+  ref_hop<true>(ctx, G, t1, out, y, c0, c1, nrhs, 0, 1);
+  return check_launch(ctx, "wl_apply_schur_normal_noalloc");
+}

@@ -39,6 +39,7 @@ EXPORTS = (
     "wl_gauge_destroy", "wl_apply", "wl_solve", "wl_engine_create", "wl_engine_destroy", "wl_engine_admit",
     "wl_engine_step", "wl_engine_poll", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
     "wl_engine_stream", "wl_engine_time_hop", "wl_kernel_launches", "wl_engine_debug_apply",
+    "wl_apply_schur_normal_noalloc",
 )
 
 
@@ -104,6 +105,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wl_engine_time_hop": (i, [vp, i, pd, pd]),
         "wl_kernel_launches": (ctypes.c_int64, []),
         "wl_engine_debug_apply": (i, [vp, i, d, vp, vp]),
+        "wl_apply_schur_normal_noalloc": (i, [vp, vp, d, u, vp, vp, i]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
