@@ -18,8 +18,7 @@ LIB = os.path.join(HERE, "_build", "libwilson_cpu.so")
 def build(force: bool = False) -> str:
     src = os.path.join(HERE, "c", "wilson_cpu.c")
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
-        # -march=native is fine: the library is rebuilt on the machine that runs it when stale
-        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "c")], check=True)
+        subprocess.run(["make", "-s", "-B" if force else "-s", "-C", os.path.join(HERE, "c")], check=True)
     return LIB
 
 
