@@ -376,6 +376,40 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile(args):
+    """Profiling driver: a fixed number of batched CG iterations of the same
+    solver, bracketed by cudaProfilerStart/Stop so that
+    `ncu --profile-from-start off` captures only those launches."""
+    import torch
+
+    from jaxqft_b200 import lib as L
+
+    global SHAPE
+    SHAPE = tuple(int(v) for v in args.shape.split(","))
+    dev = torch.device("cuda", 0)
+    ctx = L.WilsonContext(SHAPE, bc=BC, device=dev)
+    U, eta = make_inputs(torch, dev, seed=0)
+    gauge = ctx.gauge(U)
+    del U
+    b = ctx.apply("SCHUR_E_DAG", gauge, MASS, eta[:args.nrhs] * even_mask(torch, dev), normalized=True)
+    del eta
+    eng = L.Engine(ctx, gauge, args.nrhs, op="eo_normal", inner=args.inner, tol=1e-14, maxiter=100000)
+    eng.admit(np.arange(args.nrhs), b, MASS)
+    eng.step(3)
+    eng.poll()
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    t0 = time.perf_counter()
+    eng.step(args.profile_iters)
+    eng.poll()
+    t1 = time.perf_counter()
+    torch.cuda.cudart().cudaProfilerStop()
+    ms, by = eng.time_hop(reps=10)
+    print(json.dumps({"profile": "eo_normal CG iterations", "shape": SHAPE, "nrhs": args.nrhs, "inner": args.inner,
+                      "iters": args.profile_iters, "ms_per_iter_wall": (t1 - t0) * 1e3 / args.profile_iters,
+                      "hop_us": ms * 1e3, "hop_GBps": by / ms / 1e6}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -385,12 +419,19 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--fp64-all", action="store_true", help="time plain FP64 CG on all 16 RHS (default 4)")
+    ap.add_argument("--profile-iters", type=int, default=0,
+                    help="profiling driver: run this many CG iterations between cudaProfilerStart/Stop")
+    ap.add_argument("--shape", default="24,24,24,48", help="lattice for --profile-iters")
+    ap.add_argument("--nrhs", type=int, default=NRHS, help="RHS count for --profile-iters")
+    ap.add_argument("--inner", default="half", help="iterated precision for --profile-iters")
     ap.add_argument("--ref-iters", type=int, default=178,
                     help="FP64 CG iterations to 1e-10 on this system (measured by the GPU FP64 solve)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.profile_iters > 0:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -12,10 +12,12 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/wilson_sm100.h"
 #include "wl_force.cuh"
+#include "wl_hop_fast.cuh"
 #include "wl_site.cuh"
 
 using namespace wl;
@@ -94,17 +96,31 @@ struct IField {
   void* data = nullptr;
   float* norm = nullptr;
   int prec = 0, vh = 0, nrhs = 0, npar = 1;
-  long long rstride() const { return chunks_of(prec) * vh * npar; }  // chunk elements per rhs
+  bool rhs_inner = false;  // [k][Vh][nrhs] (RHS innermost) instead of [rhs][k][Vh]
+  long long rstride() const { return chunks_of(prec) * vh * npar; }  // site-major layout: chunks per rhs
 };
 
 template <int P>
 static SpinorField<P> sf(const IField& f, int par) {
   SpinorField<P> s;
   using Ptr = decltype(s.ptr);
-  s.ptr = reinterpret_cast<Ptr>(f.data) + (long long)par * chunks_of(P) * f.vh;
-  s.norm = f.norm ? f.norm + (long long)par * f.vh : nullptr;
-  s.rstride = f.rstride();
-  s.vh = f.vh;
+  const long long ch = chunks_of(P), vh = f.vh, n = f.nrhs;
+  if (!f.rhs_inner) {
+    s.ptr = reinterpret_cast<Ptr>(f.data) + par * ch * vh;
+    s.rstride = ch * vh * f.npar;
+    s.kstride = vh;
+    s.cstride = 1;
+    s.nrstride = vh;
+    s.ncstride = 1;
+  } else {
+    s.ptr = reinterpret_cast<Ptr>(f.data) + par * ch * vh * n;
+    s.rstride = 1;
+    s.kstride = vh * n;
+    s.cstride = n;
+    s.nrstride = 1;
+    s.ncstride = n;
+  }
+  s.norm = f.norm ? f.norm + par * n * vh : nullptr;
   return s;
 }
 // field pair indexed by parity; for single-parity fields both entries alias par 0
@@ -114,25 +130,12 @@ static void sf2(const IField& f, SpinorField<P> (&o)[2]) {
   o[1] = f.npar == 2 ? sf<P>(f, 1) : o[0];
 }
 
-// FP16 norm layout with npar==2: norm index rhs*vh + c must land in [rhs][par][vh]:
-// handled by giving each parity its own base and a norm stride of npar*vh.
-// To keep SpinorField simple, FP16 norms use stride vh per rhs within a parity
-// block: norm[(par * nrhs + rhs) * vh + c].
-template <>
-SpinorField<P_HALF> sf<P_HALF>(const IField& f, int par) {
-  SpinorField<P_HALF> s;
-  s.ptr = reinterpret_cast<uint4*>(f.data) + (long long)par * 3 * f.vh;
-  s.norm = f.norm + (long long)par * f.nrhs * f.vh;
-  s.rstride = f.rstride();
-  s.vh = f.vh;
-  return s;
-}
-
-static wl_status alloc_field(wl_ctx* ctx, IField& f, int prec, int vh, int nrhs, int npar) {
+static wl_status alloc_field(wl_ctx* ctx, IField& f, int prec, int vh, int nrhs, int npar, bool rhs_inner = false) {
   f.prec = prec;
   f.vh = vh;
   f.nrhs = nrhs;
   f.npar = npar;
+  f.rhs_inner = rhs_inner;
   size_t data = (size_t)chunks_of(prec) * 16 * vh * npar * nrhs;
   size_t nb = data + (prec == P_HALF ? (size_t)vh * npar * nrhs * sizeof(float) : 0);
   WL_CUDA(ctx, cudaMalloc(&f.data, nb));
@@ -161,17 +164,53 @@ static SpinorRef sref(const void* p, const Geom& g) {
 // ============================================================== launch helpers
 struct Tune {
   int nr = 1, bx = 128, by = 1;
+  int lanes = 0;  // > 0: RHS-in-lanes hop (FP16/FP32 storage) with this many RHS lanes per site
 };
 
 static dim3 grid_for(const Geom& g, const Tune& t, int nrhs, int npar) {
+  if (t.lanes > 0) {
+    const int S = kLaneBlock / t.lanes;
+    return dim3((g.Vh + S - 1) / S, (nrhs + t.lanes - 1) / t.lanes, npar);
+  }
   int groups = (nrhs + t.nr - 1) / t.nr;
   return dim3((g.Vh + t.bx - 1) / t.bx, (groups + t.by - 1) / t.by, npar);
+}
+
+template <class SF> struct UsesFastHop : std::false_type {};
+template <> struct UsesFastHop<SpinorField<P_SINGLE>> : std::true_type {};
+template <> struct UsesFastHop<SpinorField<P_HALF>> : std::true_type {};
+
+static bool fast_hop_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("WL_FAST_HOP");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 
 template <bool DAG, class IDX, class LF, class SF, class EPI>
 static void launch_hop(const Tune& t, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st) {
   dim3 grid = grid_for(a.g, t, a.nrhs, npar), block(t.bx, t.by, 1);
   g_launches++;
+  if constexpr (UsesFastHop<SF>::value && std::is_same<IDX, IdxCompact>::value) {
+    if (t.lanes > 0) {
+      dim3 lb(kLaneBlock, 1, 1);
+      switch (t.lanes) {
+        case 16: hop_lanes_kernel<DAG, 16><<<grid, lb, 0, st>>>(a); break;
+        case 8: hop_lanes_kernel<DAG, 8><<<grid, lb, 0, st>>>(a); break;
+        default: hop_lanes_kernel<DAG, 4><<<grid, lb, 0, st>>>(a); break;
+      }
+      return;
+    }
+    if (fast_hop_enabled()) {
+      switch (t.nr) {
+        case 4: hop_fast_kernel<DAG, 4><<<grid, block, 0, st>>>(a); break;
+        case 2: hop_fast_kernel<DAG, 2><<<grid, block, 0, st>>>(a); break;
+        default: hop_fast_kernel<DAG, 1><<<grid, block, 0, st>>>(a); break;
+      }
+      return;
+    }
+  }
   switch (t.nr) {
     case 4: hop_kernel<DAG, 4, IDX><<<grid, block, 0, st>>>(a); break;
     case 2: hop_kernel<DAG, 2, IDX><<<grid, block, 0, st>>>(a); break;
@@ -195,6 +234,28 @@ static void launch_site(const Tune& t, const Geom& g, int parity0, int npar, int
     case 4: site_kernel<4><<<grid, block, 0, st>>>(a); break;
     case 2: site_kernel<2><<<grid, block, 0, st>>>(a); break;
     default: site_kernel<1><<<grid, block, 0, st>>>(a); break;
+  }
+}
+
+// Site functor over (site, RHS) with RHS in the lanes (for fields in the
+// RHS-innermost layout).
+template <class F>
+static void launch_site_lanes(int R, const Geom& g, int parity0, int npar, int nrhs, const int* mask, const F& f,
+                              Reduce red, cudaStream_t st) {
+  SiteArgs<F> a;
+  a.vh = g.Vh;
+  a.parity0 = parity0;
+  a.nrhs = nrhs;
+  a.mask = mask;
+  a.f = f;
+  a.red = red;
+  const int S = kLaneBlock / R;
+  dim3 grid((g.Vh + S - 1) / S, (nrhs + R - 1) / R, npar), block(kLaneBlock, 1, 1);
+  g_launches++;
+  switch (R) {
+    case 16: site_lanes_kernel<16><<<grid, block, 0, st>>>(a); break;
+    case 8: site_lanes_kernel<8><<<grid, block, 0, st>>>(a); break;
+    default: site_lanes_kernel<4><<<grid, block, 0, st>>>(a); break;
   }
 }
 
@@ -521,6 +582,7 @@ struct wl_engine {
   int n = 0;        // slots
   int npar = 1;     // 1 for EO (even fields), 2 for full lattice
   int sprec = 0;
+  bool lanes_mode = false;  // sloppy fields RHS-innermost, sloppy hops with RHS in the lanes
   Tune ts, td, tsite;  // sloppy hop, FP64 hop, site kernels
   // fields
   IField b64, x64, y64, t64;  // FP64
@@ -564,7 +626,7 @@ int64_t engine_bytes_impl(const Geom& g, int op, int sprec, int n) {
   b += (int64_t)field_bytes(P_DOUBLE, g.Vh, n, op == WL_SOLVE_EO_NORMAL ? 1 : 2);  // t64
   b += 4 * (int64_t)field_bytes(sprec, g.Vh, n, npar);                   // xs, rs, p, y
   b += (int64_t)field_bytes(sprec, g.Vh, n, 1);                          // t1
-  b += (int64_t)n * (g.Vh / 32 + 1) * 2 * sizeof(double) + 4096;
+  b += (int64_t)n * (g.Vh / 8 + 1) * 2 * sizeof(double) + 4096;
   return b;
 }
 
@@ -587,6 +649,15 @@ static Reduce red_to(wl_engine* E, double* result) {
   r.counter = E->counters;
   r.result = result;
   return r;
+}
+
+// Site functors that touch only sloppy fields follow the sloppy layout.
+template <class F>
+static void launch_site_sloppy(wl_engine* E, int parity0, int npar, int nrhs, const int* mask, const F& f, Reduce red,
+                               cudaStream_t st) {
+  if (E->lanes_mode) launch_site_lanes(E->ts.lanes > 0 ? E->ts.lanes : 16, E->ctx->g, parity0, npar, nrhs, mask, f,
+                                       red, st);
+  else launch_site(E->tsite, E->ctx->g, parity0, npar, nrhs, mask, f, red, st);
 }
 
 __global__ void admit_state_kernel(CGScalars S, const int* admit, int use_x0, int n) {
@@ -827,7 +898,7 @@ static void enqueue_iteration(wl_engine* E, cudaStream_t st) {
     sf2<S>(E->rs, f.rs);
     sf2<S>(E->p, f.p);
     f.beta = E->beta;
-    launch_site(E->tsite, g, 0, E->npar, n, E->active, f, Reduce{}, st);
+    launch_site_sloppy(E, 0, E->npar, n, E->active, f, Reduce{}, st);
   }
 }
 
@@ -869,10 +940,10 @@ static void enqueue_admit(wl_engine* E, const void* b, int use_x0, const void* x
     FConvert<SFS, SFS> cv;
     sf2<S>(E->rs, cv.in);
     sf2<S>(E->p, cv.out);
-    launch_site(E->tsite, g, par0, E->npar, n, adm, cv, red_to(E, E->pAp), st);
+    launch_site_sloppy(E, par0, E->npar, n, adm, cv, red_to(E, E->pAp), st);
     FZero<SFS> z;
     sf2<S>(E->xs, z.out);
-    launch_site(E->tsite, g, par0, E->npar, n, adm, z, Reduce{}, st);
+    launch_site_sloppy(E, par0, E->npar, n, adm, z, Reduce{}, st);
   }
   g_launches++;
   admit_state_kernel<<<1, 128, 0, st>>>(scalars_of(E), adm, use_x0, n);
@@ -1013,6 +1084,7 @@ static Tune autotune_hop(wl_engine* E, cudaStream_t st) {
   const int n = E->n;
   std::vector<Tune> cands;
   for (int nr : {1, 2, 4}) {
+    if (E->lanes_mode) break;
     if (nr > 1 && nr > n) continue;
     int groups = (n + nr - 1) / nr;
     for (int bx : {64, 128, 256})
@@ -1020,6 +1092,15 @@ static Tune autotune_hop(wl_engine* E, cudaStream_t st) {
         if (bx * by > 256 || by * nr > kMaxRB || (by > 1 && by > groups)) continue;
         cands.push_back(Tune{nr, bx, by});
       }
+  }
+  if (E->lanes_mode) {
+    for (int lanes : {4, 8, 16}) {
+      if (lanes > n && lanes > 4) continue;
+      Tune t;
+      t.lanes = lanes;
+      t.bx = kLaneBlock;
+      cands.push_back(t);
+    }
   }
   Tune best = cands.front();
   float best_ms = 1e30f;
@@ -1056,7 +1137,21 @@ static Tune autotune_hop(wl_engine* E, cudaStream_t st) {
 }
 
 static Tune pick_tune(wl_engine* E, cudaStream_t st) {
-  TuneKey k{E->ctx->g.Vh, E->sprec, E->n, E->prm.op};
+  // WL_FORCE_TUNE="nr,bx,by,lanes" pins the hop shape (tests exercise every shape this way)
+  if (const char* f = std::getenv("WL_FORCE_TUNE")) {
+    Tune t;
+    if (std::sscanf(f, "%d,%d,%d,%d", &t.nr, &t.bx, &t.by, &t.lanes) == 4) {
+      const bool lanes_ok = t.lanes == 0 || t.lanes == 4 || t.lanes == 8 || t.lanes == 16;
+      const bool nr_ok = t.nr == 1 || t.nr == 2 || t.nr == 4;
+      const bool shape_ok = t.bx % 32 == 0 && t.bx >= 64 && t.bx * t.by <= 256 && t.by * t.nr <= kMaxRB;
+      if (lanes_ok && nr_ok && (t.lanes > 0 || shape_ok)) {
+        if (t.lanes > 0 && !E->lanes_mode) t = Tune{};  // FP64 iteration or < 4 slots: thread-per-site kernel
+        if (t.lanes > 0) t.bx = kLaneBlock;
+        return t;
+      }
+    }
+  }
+  TuneKey k{E->ctx->g.Vh, E->sprec * 2 + (E->lanes_mode ? 1 : 0), E->n, E->prm.op};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(k);
@@ -1078,8 +1173,8 @@ static Tune pick_tune(wl_engine* E, cudaStream_t st) {
   }
   const char* verb = std::getenv("WL_VERBOSE");
   if (verb && verb[0] == '1')
-    std::fprintf(stderr, "[wl] tune vh=%d prec=%d nslots=%d op=%d -> nr=%d bx=%d by=%d\n", k.vh, k.prec, k.nslots,
-                 k.op, t.nr, t.bx, t.by);
+    std::fprintf(stderr, "[wl] tune vh=%d prec=%d nslots=%d op=%d -> nr=%d bx=%d by=%d lanes=%d\n", k.vh, k.prec,
+                 k.nslots, k.op, t.nr, t.bx, t.by, t.lanes);
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune_cache[k] = t;
   return t;
@@ -1141,6 +1236,15 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   }
   const Geom& g = ctx->g;
   const int n = nslots;
+  {
+    // RHS-in-lanes sloppy hops (and the RHS-innermost field layout they need)
+    // for FP16/FP32 iteration with 4 or more slots, unless a forced shape or
+    // WL_FAST_HOP=0 selects the thread-per-site kernels
+    const char* ft = std::getenv("WL_FORCE_TUNE");
+    int fnr = 0, fbx = 0, fby = 0, flanes = -1;
+    const bool forced = ft && std::sscanf(ft, "%d,%d,%d,%d", &fnr, &fbx, &fby, &flanes) == 4;
+    E->lanes_mode = E->sprec != P_DOUBLE && n >= 4 && fast_hop_enabled() && (!forced || flanes > 0);
+  }
   wl_status s = WL_OK;
   cudaStream_t keep = ctx->stream;
   ctx->stream = st;
@@ -1149,11 +1253,12 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   if (s == WL_OK) s = alloc_field(ctx, E->x64, P_DOUBLE, g.Vh, n, E->npar);
   if (s == WL_OK) s = alloc_field(ctx, E->y64, P_DOUBLE, g.Vh, n, E->npar);
   if (s == WL_OK) s = alloc_field(ctx, E->t64, P_DOUBLE, g.Vh, n, tpar);
-  if (s == WL_OK) s = alloc_field(ctx, E->xs, E->sprec, g.Vh, n, E->npar);
-  if (s == WL_OK) s = alloc_field(ctx, E->rs, E->sprec, g.Vh, n, E->npar);
-  if (s == WL_OK) s = alloc_field(ctx, E->p, E->sprec, g.Vh, n, E->npar);
-  if (s == WL_OK) s = alloc_field(ctx, E->y, E->sprec, g.Vh, n, E->npar);
-  if (s == WL_OK) s = alloc_field(ctx, E->t1, E->sprec, g.Vh, n, 1);
+  const bool li = E->lanes_mode;
+  if (s == WL_OK) s = alloc_field(ctx, E->xs, E->sprec, g.Vh, n, E->npar, li);
+  if (s == WL_OK) s = alloc_field(ctx, E->rs, E->sprec, g.Vh, n, E->npar, li);
+  if (s == WL_OK) s = alloc_field(ctx, E->p, E->sprec, g.Vh, n, E->npar, li);
+  if (s == WL_OK) s = alloc_field(ctx, E->y, E->sprec, g.Vh, n, E->npar, li);
+  if (s == WL_OK) s = alloc_field(ctx, E->t1, E->sprec, g.Vh, n, 1, li);
   ctx->stream = keep;
   if (s != WL_OK) {
     wl_engine_destroy(E);
@@ -1161,7 +1266,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   }
   cudaError_t e = cudaMalloc(&E->dbl, sizeof(double) * kEngineDoubles * n);
   if (e == cudaSuccess) e = cudaMalloc(&E->ints, sizeof(int) * (kEngineInts * n + 1));
-  const size_t nblk = (size_t)((g.Vh + 31) / 32) * 2;
+  const size_t nblk = (size_t)((g.Vh + 7) / 8) * 2;  // smallest block: 8 sites (RHS-in-lanes hop)
   if (e == cudaSuccess) e = cudaMalloc(&E->partials, sizeof(double) * nblk * n);
   if (e == cudaSuccess) e = cudaMalloc(&E->counters, sizeof(unsigned) * (n + 1));
   if (e == cudaSuccess) e = cudaMallocHost(&E->h_pinned, sizeof(int) * (3 * n + 1));

@@ -128,85 +128,80 @@ enum Prec { P_DOUBLE = 0, P_SINGLE = 1, P_HALF = 2 };
 // Spinor field in the internal SoA compact layout.
 template <int P> struct SpinorField;
 
-template <> struct SpinorField<P_DOUBLE> {
+// Element (rhs, chunk k, site c) lives at ptr[rhs*rstride + k*kstride + c*cstride]
+// (chunk = 16 bytes).  Two layouts use this accessor:
+//   site-major   [rhs][k][Vh]: rstride = chunks*Vh*npar, kstride = Vh,   cstride = 1
+//   RHS-innermost [k][Vh][nrhs]: rstride = 1, kstride = Vh*nrhs, cstride = nrhs
+// The first coalesces when consecutive lanes are consecutive sites, the second
+// when consecutive lanes are consecutive RHS of one site.  FP16 norms use
+// norm[rhs*nrstride + c*ncstride] likewise.
+struct Strides {
+  long long rstride, kstride, cstride;
+  long long nrstride, ncstride;
+  WL_D long long at(int rhs, int k, long long c) const { return rhs * rstride + k * kstride + c * cstride; }
+  WL_D long long nat(int rhs, long long c) const { return rhs * nrstride + c * ncstride; }
+};
+
+template <> struct SpinorField<P_DOUBLE> : Strides {
   using real = double;
-  double2* ptr;       // [rhs][12][Vh]
-  float* norm;        // unused
-  long long rstride;  // elements (double2) per rhs
-  int vh;
-  WL_D void load(Spinor<double>& s, int rhs, int c) const {
-    const double2* b = ptr + rhs * rstride + c;
+  double2* ptr;
+  float* norm;  // unused
+  WL_D void load(Spinor<double>& s, int rhs, long long c) const {
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
-      double2 v = ldg(b + (long long)k * vh);
+      double2 v = ldg(ptr + at(rhs, k, c));
       s.v[k / 3][k % 3] = {v.x, v.y};
     }
   }
-  WL_D void load_plain(Spinor<double>& s, int rhs, int c) const {  // for read-after-write within a kernel
-    const double2* b = ptr + rhs * rstride + c;
+  WL_D void load_plain(Spinor<double>& s, int rhs, long long c) const {  // for read-after-write within a kernel
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
-      double2 v = b[(long long)k * vh];
+      double2 v = ptr[at(rhs, k, c)];
       s.v[k / 3][k % 3] = {v.x, v.y};
     }
   }
-  WL_D void store(const Spinor<double>& s, int rhs, int c) const {
-    double2* b = ptr + rhs * rstride + c;
+  WL_D void store(const Spinor<double>& s, int rhs, long long c) const {
 #pragma unroll
-    for (int k = 0; k < 12; ++k) b[(long long)k * vh] = make_double2(s.v[k / 3][k % 3].re, s.v[k / 3][k % 3].im);
+    for (int k = 0; k < 12; ++k) ptr[at(rhs, k, c)] = make_double2(s.v[k / 3][k % 3].re, s.v[k / 3][k % 3].im);
   }
 };
 
-template <> struct SpinorField<P_SINGLE> {
+template <> struct SpinorField<P_SINGLE> : Strides {
   using real = float;
-  float4* ptr;  // [rhs][6][Vh]
+  float4* ptr;
   float* norm;
-  long long rstride;
-  int vh;
-  WL_D void load(Spinor<float>& s, int rhs, int c) const {
-    const float4* b = ptr + rhs * rstride + c;
+  template <bool NC>
+  WL_D void load_impl(Spinor<float>& s, int rhs, long long c) const {
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      float4 v = ldg(b + (long long)k * vh);
+      float4 v = NC ? ldg(ptr + at(rhs, k, c)) : ptr[at(rhs, k, c)];
       int i0 = 2 * k, i1 = 2 * k + 1;
       s.v[i0 / 3][i0 % 3] = {v.x, v.y};
       s.v[i1 / 3][i1 % 3] = {v.z, v.w};
     }
   }
-  WL_D void load_plain(Spinor<float>& s, int rhs, int c) const {
-    const float4* b = ptr + rhs * rstride + c;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      float4 v = b[(long long)k * vh];
-      int i0 = 2 * k, i1 = 2 * k + 1;
-      s.v[i0 / 3][i0 % 3] = {v.x, v.y};
-      s.v[i1 / 3][i1 % 3] = {v.z, v.w};
-    }
-  }
-  WL_D void store(const Spinor<float>& s, int rhs, int c) const {
-    float4* b = ptr + rhs * rstride + c;
+  WL_D void load(Spinor<float>& s, int rhs, long long c) const { load_impl<true>(s, rhs, c); }
+  WL_D void load_plain(Spinor<float>& s, int rhs, long long c) const { load_impl<false>(s, rhs, c); }
+  WL_D void store(const Spinor<float>& s, int rhs, long long c) const {
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       int i0 = 2 * k, i1 = 2 * k + 1;
-      b[(long long)k * vh] = make_float4(s.v[i0 / 3][i0 % 3].re, s.v[i0 / 3][i0 % 3].im, s.v[i1 / 3][i1 % 3].re,
-                                         s.v[i1 / 3][i1 % 3].im);
+      ptr[at(rhs, k, c)] = make_float4(s.v[i0 / 3][i0 % 3].re, s.v[i0 / 3][i0 % 3].im, s.v[i1 / 3][i1 % 3].re,
+                                       s.v[i1 / 3][i1 % 3].im);
     }
   }
 };
 
-template <> struct SpinorField<P_HALF> {
+template <> struct SpinorField<P_HALF> : Strides {
   using real = float;
-  uint4* ptr;   // [rhs][3][Vh]
-  float* norm;  // [rhs][Vh]
-  long long rstride;
-  int vh;
+  uint4* ptr;
+  float* norm;
   template <bool NC>
-  WL_D void load_impl(Spinor<float>& s, int rhs, int c) const {
-    const uint4* b = ptr + rhs * rstride + c;
-    float nrm = NC ? ldg(norm + (long long)rhs * vh + c) : norm[(long long)rhs * vh + c];
+  WL_D void load_impl(Spinor<float>& s, int rhs, long long c) const {
+    float nrm = NC ? ldg(norm + nat(rhs, c)) : norm[nat(rhs, c)];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      uint4 v = NC ? ldg(b + (long long)k * vh) : b[(long long)k * vh];
+      uint4 v = NC ? ldg(ptr + at(rhs, k, c)) : ptr[at(rhs, k, c)];
       float2 a0 = h2f(v.x), a1 = h2f(v.y), a2 = h2f(v.z), a3 = h2f(v.w);
       int i = 4 * k;
       s.v[(i + 0) / 3][(i + 0) % 3] = {a0.x * nrm, a0.y * nrm};
@@ -215,9 +210,9 @@ template <> struct SpinorField<P_HALF> {
       s.v[(i + 3) / 3][(i + 3) % 3] = {a3.x * nrm, a3.y * nrm};
     }
   }
-  WL_D void load(Spinor<float>& s, int rhs, int c) const { load_impl<true>(s, rhs, c); }
-  WL_D void load_plain(Spinor<float>& s, int rhs, int c) const { load_impl<false>(s, rhs, c); }
-  WL_D void store(const Spinor<float>& s, int rhs, int c) const {
+  WL_D void load(Spinor<float>& s, int rhs, long long c) const { load_impl<true>(s, rhs, c); }
+  WL_D void load_plain(Spinor<float>& s, int rhs, long long c) const { load_impl<false>(s, rhs, c); }
+  WL_D void store(const Spinor<float>& s, int rhs, long long c) const {
     float mx = 0.f;
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -229,8 +224,7 @@ template <> struct SpinorField<P_HALF> {
     // over tens of lattice spacings.
     const bool keep = mx >= 1.17549435e-38f;
     const float inv = keep ? 1.0f / mx : 0.f;
-    norm[(long long)rhs * vh + c] = keep ? mx : 0.f;
-    uint4* b = ptr + rhs * rstride + c;
+    norm[nat(rhs, c)] = keep ? mx : 0.f;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       int i = 4 * k;
@@ -243,7 +237,7 @@ template <> struct SpinorField<P_HALF> {
       v.y = f2h(c1.re * inv, c1.im * inv);
       v.z = f2h(c2.re * inv, c2.im * inv);
       v.w = f2h(c3.re * inv, c3.im * inv);
-      b[(long long)k * vh] = v;
+      ptr[at(rhs, k, c)] = v;
     }
   }
 };

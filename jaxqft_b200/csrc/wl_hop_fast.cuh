@@ -1,0 +1,404 @@
+// Wilson hop for FP32 arithmetic (FP16 or FP32 storage) written for the
+// sm_100 packed FP32x2 pipe: every complex value is a float2 (re, im) and
+// every complex multiply-add is two __ffma2_rn:
+//     c += u * h   ==   c += (u.re, u.re) * (h.re, h.im) + (-u.im, u.im) * (h.im, h.re)
+// The FP16 per-site norm, the factor 2 of the mu=3 projector and the +-1 /
+// +-i reconstruction coefficients are folded into the accumulation weights, so
+// they cost no extra instructions.  Same contract and epilogues as hop_kernel
+// (wl_hop.cuh): acc = sum_mu [(1+cf g_mu) U psi(x+mu) + (1+cb g_mu) U^dag psi(x-mu)].
+#pragma once
+#include "wl_hop.cuh"
+
+namespace wl {
+
+WL_D float2 f2(float a, float b) { return make_float2(a, b); }
+WL_D float2 swp(float2 v) { return make_float2(v.y, v.x); }
+WL_D float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+WL_D float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
+// Raw spinor load: values without the FP16 per-site norm (returned separately).
+template <class SF> struct RawLoad;
+
+template <> struct RawLoad<SpinorField<P_SINGLE>> {
+  WL_D static float load(const SpinorField<P_SINGLE>& f, int rhs, long long c, float2 (&s)[12]) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      float4 v = ldg(f.ptr + f.at(rhs, k, c));
+      s[2 * k] = f2(v.x, v.y);
+      s[2 * k + 1] = f2(v.z, v.w);
+    }
+    return 1.0f;
+  }
+};
+
+template <> struct RawLoad<SpinorField<P_HALF>> {
+  WL_D static float load(const SpinorField<P_HALF>& f, int rhs, long long c, float2 (&s)[12]) {
+    const float n = ldg(f.norm + f.nat(rhs, c));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      uint4 v = ldg(f.ptr + f.at(rhs, k, c));
+      s[4 * k + 0] = h2f(v.x);
+      s[4 * k + 1] = h2f(v.y);
+      s[4 * k + 2] = h2f(v.z);
+      s[4 * k + 3] = h2f(v.w);
+    }
+    return n;
+  }
+};
+
+// Link as packed pairs: R[a][b] = (re, re), I[a][b] = (-im, im) of U_ab.
+struct LinkPairs {
+  float2 R[3][3], I[3][3];
+};
+
+WL_D void make_pairs(const Link<float>& u, LinkPairs& p) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      p.R[a][b] = f2(u.m[a][b].re, u.m[a][b].re);
+      p.I[a][b] = f2(-u.m[a][b].im, u.m[a][b].im);
+    }
+}
+
+// h[s*3+a], s in {0,1}: the rank-2 projection (1 + C g_mu) psi, top two rows,
+// WITHOUT the factor 2 of mu=3 (folded into the weight).
+template <int MU, int C>
+WL_D void project2(const float2 (&s)[12], float2 (&h)[6]) {
+  const float2 pc = f2((float)C, (float)C);
+  const float2 pcm = f2((float)C, -(float)C);   // for -iC x = (C x.im, -C x.re) = pcm * swap(x)
+  const float2 pmc = f2(-(float)C, (float)C);   // for  iC x = (-C x.im, C x.re) = pmc * swap(x)
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float2 s0 = s[c], s1 = s[3 + c], s2 = s[6 + c], s3 = s[9 + c];
+    if (MU == 0) {
+      h[c] = ffma2(pc, s3, s0);
+      h[3 + c] = ffma2(pc, s2, s1);
+    } else if (MU == 1) {
+      h[c] = ffma2(pcm, swp(s3), s0);      // s0 - iC s3
+      h[3 + c] = ffma2(pmc, swp(s2), s1);  // s1 + iC s2
+    } else if (MU == 2) {
+      h[c] = ffma2(pcm, swp(s2), s0);      // s0 - iC s2
+      h[3 + c] = ffma2(pcm, swp(s3), s1);  // s1 - iC s3
+    } else {
+      h[c] = C > 0 ? s0 : s2;
+      h[3 + c] = C > 0 ? s1 : s3;
+    }
+  }
+}
+
+// uh = U h (DAGU = false) or U^dag h (DAGU = true), both rows.
+template <bool DAGU>
+WL_D void color_mul2(const LinkPairs& p, const float2 (&h)[6], float2 (&uh)[6]) {
+#pragma unroll
+  for (int sp = 0; sp < 2; ++sp) {
+    float2 hs[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) hs[b] = swp(h[sp * 3 + b]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float2 acc = f2(0.f, 0.f);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        if (DAGU) {  // conj(U_ba): (re, re) h + (im, -im) swap(h)
+          acc = ffma2(p.R[b][a], h[sp * 3 + b], acc);
+          acc = ffma2(f2(-p.I[b][a].x, -p.I[b][a].y), hs[b], acc);
+        } else {
+          acc = ffma2(p.R[a][b], h[sp * 3 + b], acc);
+          acc = ffma2(p.I[a][b], hs[b], acc);
+        }
+      }
+      uh[sp * 3 + a] = acc;
+    }
+  }
+}
+
+// acc += w * full spinor reconstructed from uh (rows 0,1 = uh; rows 2,3 by MU, C).
+template <int MU, int C>
+WL_D void accum2(float2 (&acc)[12], const float2 (&uh)[6], float w) {
+  const float2 ww = f2(w, w);
+  const float2 cw = f2(C * w, C * w);
+  const float2 pcm = f2(C * w, -C * w);   // -iC w x = pcm * swap(x)
+  const float2 pmc = f2(-C * w, C * w);   //  iC w x = pmc * swap(x)
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float2 u0 = uh[c], u1 = uh[3 + c];
+    if (MU == 3) {
+      if (C > 0) {
+        acc[c] = ffma2(ww, u0, acc[c]);
+        acc[3 + c] = ffma2(ww, u1, acc[3 + c]);
+      } else {
+        acc[6 + c] = ffma2(ww, u0, acc[6 + c]);
+        acc[9 + c] = ffma2(ww, u1, acc[9 + c]);
+      }
+      continue;
+    }
+    acc[c] = ffma2(ww, u0, acc[c]);
+    acc[3 + c] = ffma2(ww, u1, acc[3 + c]);
+    if (MU == 0) {
+      acc[6 + c] = ffma2(cw, u1, acc[6 + c]);
+      acc[9 + c] = ffma2(cw, u0, acc[9 + c]);
+    } else if (MU == 1) {
+      acc[6 + c] = ffma2(pcm, swp(u1), acc[6 + c]);  // -iC u1
+      acc[9 + c] = ffma2(pmc, swp(u0), acc[9 + c]);  //  iC u0
+    } else {
+      acc[6 + c] = ffma2(pmc, swp(u0), acc[6 + c]);  //  iC u0
+      acc[9 + c] = ffma2(pmc, swp(u1), acc[9 + c]);  //  iC u1
+    }
+  }
+}
+
+template <int MU, bool DAG, int NR, class LF, class SF>
+WL_D void hop_dir_fast(const Geom& g, const LF& links, const SF& src, int parity, const Site& s, int rhs0,
+                       const bool (&act)[NR], float2 (&acc)[NR][12]) {
+  constexpr int CF = DAG ? +1 : -1;
+  constexpr int CB = -CF;
+  constexpr float W3 = (MU == 3) ? 2.0f : 1.0f;
+#pragma unroll
+  for (int dir = 0; dir < 2; ++dir) {
+    const long long nb = neighbor(g, s, MU, dir == 0 ? +1 : -1);
+    Link<float> u;
+    if (dir == 0) links.load(u, parity, MU, s.c);
+    else links.load(u, 1 - parity, MU, nb);
+    LinkPairs lp;
+    make_pairs(u, lp);
+    const bool ph = g.ph_on[MU] && (dir == 0 ? (s.x[MU] == g.L[MU] - 1) : (s.x[MU] == 0));
+    const float phr = (float)g.ph_re[MU], phi = dir == 0 ? (float)g.ph_im[MU] : -(float)g.ph_im[MU];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      if (!act[r]) continue;
+      float2 sp[12];
+      const float n = RawLoad<SF>::load(src, rhs0 + r, nb, sp) * W3;
+      float2 h[6], uh[6];
+      if (dir == 0) {
+        project2<MU, CF>(sp, h);
+        color_mul2<false>(lp, h, uh);
+      } else {
+        project2<MU, CB>(sp, h);
+        color_mul2<true>(lp, h, uh);
+      }
+      if (ph) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) uh[k] = ffma2(f2(phr, phr), uh[k], fmul2(f2(-phi, phi), swp(uh[k])));
+      }
+      if (dir == 0) accum2<MU, CF>(acc[r], uh, n);
+      else accum2<MU, CB>(acc[r], uh, n);
+    }
+  }
+}
+
+template <bool DAG, int NR, class LF, class SF, class EPI>
+__global__ void __launch_bounds__(256) hop_fast_kernel(HopArgs<LF, SF, EPI> A) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int parity = A.parity0 ^ blockIdx.z;
+  const int rhs0 = (blockIdx.y * blockDim.y + threadIdx.y) * NR;
+  double red[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) red[r] = 0.0;
+  if (c < A.g.Vh) {
+    bool act[NR];
+    bool any = false;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      act[r] = (rhs0 + r < A.nrhs) && (A.mask == nullptr || A.mask[rhs0 + r] != 0);
+      any |= act[r];
+    }
+    if (any) {
+      const Site s = site_from_compact(A.g, parity, c);
+      float2 acc[NR][12];
+#pragma unroll
+      for (int r = 0; r < NR; ++r)
+#pragma unroll
+        for (int k = 0; k < 12; ++k) acc[r][k] = f2(0.f, 0.f);
+      const SF& src = A.src[1 - parity];
+      hop_dir_fast<0, DAG, NR>(A.g, A.links, src, parity, s, rhs0, act, acc);
+      hop_dir_fast<1, DAG, NR>(A.g, A.links, src, parity, s, rhs0, act, acc);
+      hop_dir_fast<2, DAG, NR>(A.g, A.links, src, parity, s, rhs0, act, acc);
+      hop_dir_fast<3, DAG, NR>(A.g, A.links, src, parity, s, rhs0, act, acc);
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        if (!act[r]) continue;
+        Spinor<float> o;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) o.v[k / 3][k % 3] = {acc[r][k].x, acc[r][k].y};
+        red[r] = A.epi(rhs0 + r, parity, (long long)c, o);
+      }
+    }
+  }
+  if (EPI::kReduce) reduce_rhs<NR>(red, A.red, A.nrhs, A.mask);
+}
+
+// ============================================================================
+// Multi-RHS hop with RHS in the lanes.  A block of 128 threads covers
+// S = 128 / R sites x R right-hand sides (lane = rhs + R * site).  Phase 1: the
+// block reconstructs the 8 links of each of its sites once into shared memory
+// as packed pairs (boundary phase folded in) together with the neighbour
+// indices.  Phase 2: every lane runs the stencil for its (site, RHS), reading
+// the site's links as shared-memory broadcasts.  Spinor loads stay
+// sector-efficient: lanes r of sites c and c+1 read the two 16-byte halves of
+// one 32-byte sector.
+constexpr int kLaneBlock = 128;
+
+struct LinkSmem {
+  float4 p[9];  // (R.x, R.y, I.x, I.y) for element (a, b) = k / 3, k % 3
+};
+
+// One site's 8 links; the 16-byte pad makes the per-site stride 1168 B so the
+// sites read by one warp fall in different shared-memory banks.
+struct SiteLinks {
+  LinkSmem l[8];  // q = 2*mu + dir
+  float4 pad;
+};
+
+template <int R>
+struct LaneSmem {
+  static constexpr int S = kLaneBlock / R;
+  SiteLinks link[S];
+  int nb[S][8];
+  int ok[S];
+};
+
+template <bool DAGU>
+WL_D void color_mul_smem(const LinkSmem& L, const float2 (&h)[6], float2 (&uh)[6]) {
+#pragma unroll
+  for (int sp = 0; sp < 2; ++sp) {
+    float2 hs[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) hs[b] = swp(h[sp * 3 + b]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float2 acc = f2(0.f, 0.f);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const float4 q = DAGU ? L.p[b * 3 + a] : L.p[a * 3 + b];
+        acc = ffma2(f2(q.x, q.y), h[sp * 3 + b], acc);
+        acc = DAGU ? ffma2(f2(-q.z, -q.w), hs[b], acc) : ffma2(f2(q.z, q.w), hs[b], acc);
+      }
+      uh[sp * 3 + a] = acc;
+    }
+  }
+}
+
+template <int MU, bool DAG, class SF>
+WL_D void lane_dir(const SF& src, const LinkSmem* Ls, const int* nbs, int rhs, float2 (&acc)[12]) {
+  constexpr int CF = DAG ? +1 : -1;
+  constexpr int CB = -CF;
+  constexpr float W3 = (MU == 3) ? 2.0f : 1.0f;
+#pragma unroll
+  for (int dir = 0; dir < 2; ++dir) {
+    const int q = 2 * MU + dir;
+    float2 sp[12];
+    const float n = RawLoad<SF>::load(src, rhs, (long long)nbs[q], sp) * W3;
+    float2 h[6], uh[6];
+    if (dir == 0) {
+      project2<MU, CF>(sp, h);
+      color_mul_smem<false>(Ls[q], h, uh);
+      accum2<MU, CF>(acc, uh, n);
+    } else {
+      project2<MU, CB>(sp, h);
+      color_mul_smem<true>(Ls[q], h, uh);
+      accum2<MU, CB>(acc, uh, n);
+    }
+  }
+}
+
+template <int R>
+WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* mask) {
+  __shared__ double sw[kLaneBlock / 32][32];
+  __shared__ int s_last;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int off = R; off < 32; off <<= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if (lane < R) sw[warp][lane] = v;
+  __syncthreads();
+  const int nblk = gridDim.x * gridDim.z;
+  const int blk = blockIdx.z * gridDim.x + blockIdx.x;
+  const int rbase = blockIdx.y * R;
+  if (tid < R) {
+    double x = 0.0;
+#pragma unroll
+    for (int w = 0; w < kLaneBlock / 32; ++w) x += sw[w][tid];
+    if (rbase + tid < nrhs) Rd.partials[(long long)(rbase + tid) * nblk + blk] = x;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    unsigned t = atomicAdd(&Rd.counter[blockIdx.y], 1u);
+    s_last = (t == (unsigned)nblk - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double* sred = &sw[0][0];
+  for (int i = 0; i < R; ++i) {
+    const int rhs = rbase + i;
+    if (rhs >= nrhs) break;
+    double vv[1] = {0.0};
+    for (int b = tid; b < nblk; b += kLaneBlock) vv[0] += __ldcg(&Rd.partials[(long long)rhs * nblk + b]);
+    block_sum<1>(vv, sred);
+    if (tid == 0 && (mask == nullptr || mask[rhs] != 0)) Rd.result[rhs] = vv[0];
+    __syncthreads();
+  }
+  if (tid == 0) Rd.counter[blockIdx.y] = 0;
+}
+
+template <bool DAG, int R, class LF, class SF, class EPI>
+__global__ void __launch_bounds__(kLaneBlock) hop_lanes_kernel(HopArgs<LF, SF, EPI> A) {
+  constexpr int S = kLaneBlock / R;
+  __shared__ LaneSmem<R> sm;
+  const int tid = threadIdx.x;
+  const int parity = A.parity0 ^ blockIdx.z;
+  const int site0 = blockIdx.x * S;
+  // ---- phase 1: links (phase-folded packed pairs) and neighbour indices
+  for (int j = tid; j < 8 * S; j += kLaneBlock) {
+    const int sl = j >> 3, q = j & 7, mu = q >> 1, dir = q & 1;
+    const int c = site0 + sl;
+    if (c < A.g.Vh) {
+      const Site s = site_from_compact(A.g, parity, c);
+      const int nb = neighbor(A.g, s, mu, dir == 0 ? +1 : -1);
+      Link<float> u;
+      if (dir == 0) A.links.load(u, parity, mu, c);
+      else A.links.load(u, 1 - parity, mu, nb);
+      // the forward hop from x_mu = L-1 uses ph*U; the backward hop into
+      // x_mu = 0 uses (ph*U)^dag, i.e. the same phase-multiplied link
+      const bool ph = A.g.ph_on[mu] && (dir == 0 ? (s.x[mu] == A.g.L[mu] - 1) : (s.x[mu] == 0));
+      const float pr = ph ? (float)A.g.ph_re[mu] : 1.f, pi = ph ? (float)A.g.ph_im[mu] : 0.f;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const cplx<float> v = u.m[k / 3][k % 3] * cplx<float>{pr, pi};
+        sm.link[sl].l[q].p[k] = make_float4(v.re, v.re, -v.im, v.im);
+      }
+      sm.nb[sl][q] = nb;
+      if (q == 0) sm.ok[sl] = 1;
+    } else if (q == 0) {
+      sm.ok[sl] = 0;
+    }
+  }
+  __syncthreads();
+  // ---- phase 2: stencil for (site, rhs) of this lane
+  const int sl = tid / R;
+  const int c = site0 + sl;
+  const int rhs = blockIdx.y * R + (tid % R);
+  double red = 0.0;
+  const bool act = sm.ok[sl] && rhs < A.nrhs && (A.mask == nullptr || A.mask[rhs] != 0);
+  if (act) {
+    float2 acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = f2(0.f, 0.f);
+    const SF& src = A.src[1 - parity];
+    const LinkSmem* Ls = sm.link[sl].l;
+    const int* nbs = sm.nb[sl];
+    lane_dir<0, DAG>(src, Ls, nbs, rhs, acc);
+    lane_dir<1, DAG>(src, Ls, nbs, rhs, acc);
+    lane_dir<2, DAG>(src, Ls, nbs, rhs, acc);
+    lane_dir<3, DAG>(src, Ls, nbs, rhs, acc);
+    Spinor<float> o;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) o.v[k / 3][k % 3] = {acc[k].x, acc[k].y};
+    red = A.epi(rhs, parity, (long long)c, o);
+  }
+  if (EPI::kReduce) reduce_lanes<R>(red, A.red, A.nrhs, A.mask);
+}
+
+}  // namespace wl

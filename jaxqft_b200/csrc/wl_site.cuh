@@ -1,7 +1,7 @@
 // Site-local kernels: layout conversion (reference <-> internal), precision
 // conversion, gauge-field compression and the CG vector/scalar updates.
 #pragma once
-#include "wl_hop.cuh"
+#include "wl_hop_fast.cuh"
 
 namespace wl {
 
@@ -29,6 +29,20 @@ __global__ void __launch_bounds__(256) site_kernel(SiteArgs<F> A) {
     if (c < A.vh && rhs < A.nrhs && (A.mask == nullptr || A.mask[rhs] != 0)) red[r] = A.f(rhs, parity, c);
   }
   if (F::kReduce) reduce_rhs<NR>(red, A.red, A.nrhs, A.mask);
+}
+
+// Same functors with RHS in the lanes: lane = rhs + R * site (fields in the
+// RHS-innermost layout coalesce this way).
+template <int R, class F>
+__global__ void __launch_bounds__(kLaneBlock) site_lanes_kernel(SiteArgs<F> A) {
+  constexpr int S = kLaneBlock / R;
+  const int tid = threadIdx.x;
+  const int c = blockIdx.x * S + tid / R;
+  const int rhs = blockIdx.y * R + (tid % R);
+  const int parity = A.parity0 ^ blockIdx.z;
+  double red = 0.0;
+  if (c < A.vh && rhs < A.nrhs && (A.mask == nullptr || A.mask[rhs] != 0)) red = A.f(rhs, parity, c);
+  if (F::kReduce) reduce_lanes<R>(red, A.red, A.nrhs, A.mask);
 }
 
 // -------------------------------------------------------- layout conversion

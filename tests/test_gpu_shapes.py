@@ -1,0 +1,83 @@
+"""Every hop kernel shape the autotuner can choose, pinned with WL_FORCE_TUNE:
+classic thread-per-site kernels with 1/2/4 RHS per thread and the RHS-in-lanes
+kernel with 4/8/16 lanes per site.  Each shape must give the same operator
+(FP32: 2e-6, FP16: 4e-3 of FP64) and batched solves that reach an FP64 true
+residual <= 1e-10 and agree with standalone FP64 solves."""
+
+import os
+
+import numpy as np
+import pytest
+
+from oracle import wilson as W
+from tests.conftest import rel
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("CUDA device required", allow_module_level=True)
+
+from jaxqft_b200.lib import Engine, WilsonContext  # noqa: E402
+
+SHAPES = ["1,128,1,0", "2,64,2,0", "4,64,4,0", "1,128,1,4", "1,128,1,8", "1,128,1,16"]
+TOLS = {"single": 2e-6, "half": 4e-3}
+
+
+@pytest.fixture(scope="module")
+def setup():
+    shape = (4, 6, 4, 8)
+    rng = np.random.default_rng(31)
+    U = W.hot_links(rng, shape, 1, 0.2)
+    bc = (1, 1, 1j, -1)
+    ctx = WilsonContext(shape, bc=bc)
+    gauge = ctx.gauge(torch.from_numpy(U[0]))
+    return shape, U, bc, ctx, gauge, rng
+
+
+@pytest.fixture
+def forced(request):
+    os.environ["WL_FORCE_TUNE"] = request.param
+    yield request.param
+    del os.environ["WL_FORCE_TUNE"]
+
+
+@pytest.mark.parametrize("forced", SHAPES, indirect=True)
+@pytest.mark.parametrize("inner", ["single", "half"])
+def test_operator_per_shape(setup, forced, inner):
+    shape, U, bc, ctx, gauge, rng = setup
+    m = -0.25
+    eng = Engine(ctx, gauge, 16, op="eo_normal", inner=inner)
+    xe = W.project(W.gaussian_spinor(rng, shape, 1), 0)
+    s = W.schur_even(U, xe, m, bc, normalized=True)
+    ref = W.schur_even(U, s, m, bc, normalized=True, dag=True)
+    out = eng.debug_apply(2, m, torch.from_numpy(xe[0])).cpu().numpy()
+    assert rel(out, ref[0]) < TOLS[inner], (forced, inner)
+    eng.close()
+    eng = Engine(ctx, gauge, 16, op="normal", inner=inner)
+    x = W.gaussian_spinor(rng, shape, 1)
+    out = eng.debug_apply(4, m, torch.from_numpy(x[0])).cpu().numpy()
+    assert rel(out, W.apply_normal(U, x, m, bc)[0]) < TOLS[inner], (forced, inner)
+    eng.close()
+
+
+@pytest.mark.parametrize("forced", SHAPES, indirect=True)
+def test_batched_solve_per_shape(setup, forced):
+    shape, U, bc, ctx, gauge, rng = setup
+    n = 13  # not a multiple of any lane / RHS-block count
+    masses = np.linspace(-0.3, 0.1, n)
+    b = W.project(W.gaussian_spinor(rng, shape, n), 0)
+    b[5] *= 1e-4
+    eng = Engine(ctx, gauge, n, op="eo_normal", inner="half", tol=1e-10, maxiter=3000)
+    eng.admit(np.arange(n), torch.from_numpy(b), masses)
+    na = n
+    while na:
+        eng.step(8)
+        _, na = eng.poll()
+    for r in range(n):
+        x, st = eng.retire(r)
+        assert st["status"] == 2, (forced, r, st)
+        x = x.cpu().numpy()
+        s = W.schur_even(U, x[None], masses[r], bc, normalized=True)
+        ax = W.schur_even(U, s, masses[r], bc, normalized=True, dag=True)[0]
+        assert np.linalg.norm(b[r] - ax) / np.linalg.norm(b[r]) <= 1e-10, (forced, r)
+    eng.close()
