@@ -393,7 +393,8 @@ def run_profile(args):
     del U
     b = ctx.apply("SCHUR_E_DAG", gauge, MASS, eta[:args.nrhs] * even_mask(torch, dev), normalized=True)
     del eta
-    eng = L.Engine(ctx, gauge, args.nrhs, op="eo_normal", inner=args.inner, tol=1e-14, maxiter=100000)
+    eng = L.Engine(ctx, gauge, args.nrhs, op="eo_normal", inner=args.inner, tol=1e-14, maxiter=100000,
+                   use_graph=not args.no_graph)
     eng.admit(np.arange(args.nrhs), b, MASS)
     eng.step(3)
     eng.poll()
@@ -424,6 +425,9 @@ def main():
     ap.add_argument("--shape", default="24,24,24,48", help="lattice for --profile-iters")
     ap.add_argument("--nrhs", type=int, default=NRHS, help="RHS count for --profile-iters")
     ap.add_argument("--inner", default="half", help="iterated precision for --profile-iters")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="--profile-iters: launch kernels directly (ncu cannot profile kernels inside graphs "
+                         "with conditional nodes)")
     ap.add_argument("--ref-iters", type=int, default=178,
                     help="FP64 CG iterations to 1e-10 on this system (measured by the GPU FP64 solve)")
     args = ap.parse_args()

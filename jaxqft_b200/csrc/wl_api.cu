@@ -188,8 +188,27 @@ static bool fast_hop_enabled() {
   return on;
 }
 
+// `per_block`: partial sums each block writes per RHS (lane kernels: one per warp)
+static void launch_finalize(const Reduce& r, int nrhs, dim3 grid, const int* mask, cudaStream_t st,
+                            int per_block = 1) {
+  g_launches++;
+  reduce_finalize_kernel<<<nrhs, kFinalizeThreads, 0, st>>>(r, nrhs, (int)(grid.x * grid.z) * per_block, mask);
+}
+
+template <bool DAG, class IDX, class LF, class SF, class EPI>
+static void launch_hop_impl(const Tune& t, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st);
+
 template <bool DAG, class IDX, class LF, class SF, class EPI>
 static void launch_hop(const Tune& t, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st) {
+  launch_hop_impl<DAG, IDX>(t, a, npar, st);
+  if (EPI::kReduce) {
+    const bool lanes = UsesFastHop<SF>::value && std::is_same<IDX, IdxCompact>::value && t.lanes > 0;
+    launch_finalize(a.red, a.nrhs, grid_for(a.g, t, a.nrhs, npar), a.mask, st, lanes ? kLaneWarps : 1);
+  }
+}
+
+template <bool DAG, class IDX, class LF, class SF, class EPI>
+static void launch_hop_impl(const Tune& t, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st) {
   dim3 grid = grid_for(a.g, t, a.nrhs, npar), block(t.bx, t.by, 1);
   g_launches++;
   if constexpr (UsesFastHop<SF>::value && std::is_same<IDX, IdxCompact>::value) {
@@ -235,6 +254,7 @@ static void launch_site(const Tune& t, const Geom& g, int parity0, int npar, int
     case 2: site_kernel<2><<<grid, block, 0, st>>>(a); break;
     default: site_kernel<1><<<grid, block, 0, st>>>(a); break;
   }
+  if (F::kReduce) launch_finalize(red, nrhs, grid, mask, st);
 }
 
 // Site functor over (site, RHS) with RHS in the lanes (for fields in the
@@ -257,6 +277,7 @@ static void launch_site_lanes(int R, const Geom& g, int parity0, int npar, int n
     case 8: site_lanes_kernel<8><<<grid, block, 0, st>>>(a); break;
     default: site_lanes_kernel<4><<<grid, block, 0, st>>>(a); break;
   }
+  if (F::kReduce) launch_finalize(red, nrhs, grid, mask, st, kLaneWarps);
 }
 
 // ============================================================== context
@@ -602,7 +623,13 @@ struct wl_engine {
   // graph
   cudaGraphExec_t gexec = nullptr;
   bool graph_built = false;
-  long long graph_kernels = 0;  // kernel nodes per captured iteration
+  long long graph_kernels = 0;     // unconditional kernel nodes per captured iteration
+  long long ru_body_kernels = 0;   // kernels in the conditional reliable-update body
+  bool use_cond = false;           // decide kernel drives a graph conditional node
+  cudaGraphConditionalHandle cond = 0;
+  int* ru_iters = nullptr;         // device: iterations whose conditional body ran
+  long long ru_iters_seen = 0;
+  bool ru_links12 = false;         // FP64 true residual with 12-real links (links unitary to 1e-12)
 };
 
 struct EngineStream {
@@ -626,7 +653,7 @@ int64_t engine_bytes_impl(const Geom& g, int op, int sprec, int n) {
   b += (int64_t)field_bytes(P_DOUBLE, g.Vh, n, op == WL_SOLVE_EO_NORMAL ? 1 : 2);  // t64
   b += 4 * (int64_t)field_bytes(sprec, g.Vh, n, npar);                   // xs, rs, p, y
   b += (int64_t)field_bytes(sprec, g.Vh, n, 1);                          // t1
-  b += (int64_t)n * (g.Vh / 8 + 1) * 2 * sizeof(double) + 4096;
+  b += (int64_t)n * (g.Vh + 64) * sizeof(double) + 4096;
   return b;
 }
 
@@ -771,35 +798,34 @@ static void time_hop_impl(wl_engine* E, cudaStream_t st, int reps, float* ms) {
 
 // Enqueue the FP64 normal operator on x64 ending in the true residual
 // rs = convert(b - A x64), r2_true = |b - A x64|^2, for the slots in `mask`.
-template <int S>
-static void enqueue_true_residual(wl_engine* E, const int* mask, cudaStream_t st) {
+template <int S, class LDT>
+static void enqueue_true_residual_links(wl_engine* E, const int* mask, cudaStream_t st, const LDT& LD) {
   using SFS = SpinorField<S>;
   using SFD = SpinorField<P_DOUBLE>;
   const Geom& g = E->ctx->g;
-  LinkField<L_D18> LD{E->gauge->d18, g.Vh};
   const bool eo = E->prm.op == WL_SOLVE_EO_NORMAL;
   if (eo) {
     {  // t64 = K_oe x64
-      HopArgs<LinkField<L_D18>, SFD, EpiXpay<SFD, false>> A{};
+      HopArgs<LDT, SFD, EpiXpay<SFD, false>> A{};
       A.g = g; A.links = LD; sf2<P_DOUBLE>(E->x64, A.src); A.parity0 = 1; A.nrhs = E->n; A.mask = mask;
       sf2<P_DOUBLE>(E->t64, A.epi.out); A.epi.has_self = 0; A.epi.b = E->neg_half;
       launch_hop<false, IdxCompact>(E->td, A, 1, st);
     }
     {  // y64 = x64 + (alpha/2) hop(t64)
-      HopArgs<LinkField<L_D18>, SFD, EpiXpay<SFD, false>> A{};
+      HopArgs<LDT, SFD, EpiXpay<SFD, false>> A{};
       A.g = g; A.links = LD; sf2<P_DOUBLE>(E->t64, A.src); A.parity0 = 0; A.nrhs = E->n; A.mask = mask;
       sf2<P_DOUBLE>(E->y64, A.epi.out); sf2<P_DOUBLE>(E->x64, A.epi.self); A.epi.has_self = 1;
       A.epi.a = E->one; A.epi.b = E->half_alpha;
       launch_hop<false, IdxCompact>(E->td, A, 1, st);
     }
     {  // t64 = Kdag_oe y64
-      HopArgs<LinkField<L_D18>, SFD, EpiXpay<SFD, false>> A{};
+      HopArgs<LDT, SFD, EpiXpay<SFD, false>> A{};
       A.g = g; A.links = LD; sf2<P_DOUBLE>(E->y64, A.src); A.parity0 = 1; A.nrhs = E->n; A.mask = mask;
       sf2<P_DOUBLE>(E->t64, A.epi.out); A.epi.has_self = 0; A.epi.b = E->neg_half;
       launch_hop<true, IdxCompact>(E->td, A, 1, st);
     }
     {  // rs = b - (y64 + (alpha/2) hopdag(t64))
-      HopArgs<LinkField<L_D18>, SFD, EpiResid<SFS>> A{};
+      HopArgs<LDT, SFD, EpiResid<SFS>> A{};
       A.g = g; A.links = LD; sf2<P_DOUBLE>(E->t64, A.src); A.parity0 = 0; A.nrhs = E->n; A.mask = mask;
       sf2<P_DOUBLE>(E->y64, A.epi.y); sf2<P_DOUBLE>(E->b64, A.epi.bvec); sf2<S>(E->rs, A.epi.rs);
       A.epi.a = E->one; A.epi.b = E->half_alpha;
@@ -808,14 +834,14 @@ static void enqueue_true_residual(wl_engine* E, const int* mask, cudaStream_t st
     }
   } else {
     {  // y64 = D x64
-      HopArgs<LinkField<L_D18>, SFD, EpiXpay<SFD, false>> A{};
+      HopArgs<LDT, SFD, EpiXpay<SFD, false>> A{};
       A.g = g; A.links = LD; sf2<P_DOUBLE>(E->x64, A.src); A.parity0 = 0; A.nrhs = E->n; A.mask = mask;
       sf2<P_DOUBLE>(E->y64, A.epi.out); sf2<P_DOUBLE>(E->x64, A.epi.self); A.epi.has_self = 1;
       A.epi.a = E->m0; A.epi.b = E->neg_half;
       launch_hop<false, IdxCompact>(E->td, A, 2, st);
     }
     {  // rs = b - D^dag y64
-      HopArgs<LinkField<L_D18>, SFD, EpiResid<SFS>> A{};
+      HopArgs<LDT, SFD, EpiResid<SFS>> A{};
       A.g = g; A.links = LD; sf2<P_DOUBLE>(E->y64, A.src); A.parity0 = 0; A.nrhs = E->n; A.mask = mask;
       sf2<P_DOUBLE>(E->y64, A.epi.y); sf2<P_DOUBLE>(E->b64, A.epi.bvec); sf2<S>(E->rs, A.epi.rs);
       A.epi.a = E->m0; A.epi.b = E->neg_half;
@@ -825,15 +851,47 @@ static void enqueue_true_residual(wl_engine* E, const int* mask, cudaStream_t st
   }
 }
 
-// One CG iteration for all active slots.
 template <int S>
-static void enqueue_iteration(wl_engine* E, cudaStream_t st) {
+static void enqueue_true_residual(wl_engine* E, const int* mask, cudaStream_t st) {
+  const Geom& g = E->ctx->g;
+  if (E->ru_links12) enqueue_true_residual_links<S>(E, mask, st, LinkField<L_D12>{E->gauge->d12, g.Vh});
+  else enqueue_true_residual_links<S>(E, mask, st, LinkField<L_D18>{E->gauge->d18, g.Vh});
+}
+
+// One CG iteration for all active slots, in three parts: (1) the sloppy
+// normal operator with the fused CG update and the reliable-update decision,
+// (2) the reliable update (x += x_s; r = b - A x in FP64) for the slots that
+// take one, (3) convergence bookkeeping and p = r + beta p.  In a CUDA graph,
+// part 2 sits in a conditional node that runs only when some slot needs it.
+template <int S>
+static void enqueue_iteration(wl_engine* E, cudaStream_t st, int part) {
   using SFS = SpinorField<S>;
   using LS = typename SloppyLinks<S>::type;
   const Geom& g = E->ctx->g;
   LS L = SloppyLinks<S>::get(E->gauge);
   const bool eo = E->prm.op == WL_SOLVE_EO_NORMAL;
   const int n = E->n;
+  CGScalars Sc = scalars_of(E);
+  if (part == 2) {
+    {  // x64 += xs ; xs = 0  (reliable-update slots)
+      FAccumX<SFS> f;
+      sf2<P_DOUBLE>(E->x64, f.x);
+      sf2<S>(E->xs, f.xs);
+      launch_site(E->tsite, g, 0, E->npar, n, E->ru, f, Reduce{}, st);
+    }
+    enqueue_true_residual<S>(E, E->ru, st);
+    return;
+  }
+  if (part == 3) {
+    g_launches++;
+    cg_finalize_kernel<<<1, 128, 0, st>>>(Sc, n);
+    FUpdateP<SFS> f;  // p = rs + beta p
+    sf2<S>(E->rs, f.rs);
+    sf2<S>(E->p, f.p);
+    f.beta = E->beta;
+    launch_site_sloppy(E, 0, E->npar, n, E->active, f, Reduce{}, st);
+    return;
+  }
   if (eo) {
     {  // t1 = K_oe p
       HopArgs<LS, SFS, EpiXpay<SFS, false>> A{};
@@ -881,25 +939,8 @@ static void enqueue_iteration(wl_engine* E, cudaStream_t st) {
       launch_hop<true, IdxCompact>(E->ts, A, 2, st);
     }
   }
-  CGScalars Sc = scalars_of(E);
   g_launches++;
-  cg_decide_kernel<<<1, 128, 0, st>>>(Sc, n);
-  {  // x64 += xs ; xs = 0  (reliable-update slots)
-    FAccumX<SFS> f;
-    sf2<P_DOUBLE>(E->x64, f.x);
-    sf2<S>(E->xs, f.xs);
-    launch_site(E->tsite, g, 0, E->npar, n, E->ru, f, Reduce{}, st);
-  }
-  enqueue_true_residual<S>(E, E->ru, st);
-  g_launches++;
-  cg_finalize_kernel<<<1, 128, 0, st>>>(Sc, n);
-  {  // p = rs + beta p
-    FUpdateP<SFS> f;
-    sf2<S>(E->rs, f.rs);
-    sf2<S>(E->p, f.p);
-    f.beta = E->beta;
-    launch_site_sloppy(E, 0, E->npar, n, E->active, f, Reduce{}, st);
-  }
+  cg_decide_kernel<<<1, 128, 0, st>>>(Sc, n, E->use_cond ? 1 : 0, E->cond, E->use_cond ? E->ru_iters : nullptr);
 }
 
 template <int S>
@@ -1064,12 +1105,18 @@ extern "C" wl_status wl_engine_debug_apply(wl_engine* E, int stage, double mass,
   return check_launch(ctx, "wl_engine_debug_apply");
 }
 
-static void enqueue_iteration_any(wl_engine* E, cudaStream_t st) {
+static void enqueue_part(wl_engine* E, cudaStream_t st, int part) {
   switch (E->sprec) {
-    case P_HALF: enqueue_iteration<P_HALF>(E, st); break;
-    case P_SINGLE: enqueue_iteration<P_SINGLE>(E, st); break;
-    default: enqueue_iteration<P_DOUBLE>(E, st); break;
+    case P_HALF: enqueue_iteration<P_HALF>(E, st, part); break;
+    case P_SINGLE: enqueue_iteration<P_SINGLE>(E, st, part); break;
+    default: enqueue_iteration<P_DOUBLE>(E, st, part); break;
   }
+}
+
+static void enqueue_iteration_any(wl_engine* E, cudaStream_t st) {
+  enqueue_part(E, st, 1);
+  enqueue_part(E, st, 2);
+  enqueue_part(E, st, 3);
 }
 
 // ------------------------------------------------------------------ autotune
@@ -1193,6 +1240,7 @@ extern "C" void wl_engine_destroy(wl_engine* E) {
   cudaFree(E->ints);
   cudaFree(E->partials);
   cudaFree(E->counters);
+  cudaFree(E->ru_iters);
   if (E->h_pinned) cudaFreeHost(E->h_pinned);
   if (st) cudaStreamDestroy(st);
   {
@@ -1228,6 +1276,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
     return s0;
   }
   if (E->sprec != P_DOUBLE && !(uerr < 1e-4)) E->sprec = P_DOUBLE;
+  E->ru_links12 = uerr < 1e-12;
   cudaStream_t st;
   WL_CUDA(ctx, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   {
@@ -1266,10 +1315,13 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   }
   cudaError_t e = cudaMalloc(&E->dbl, sizeof(double) * kEngineDoubles * n);
   if (e == cudaSuccess) e = cudaMalloc(&E->ints, sizeof(int) * (kEngineInts * n + 1));
-  const size_t nblk = (size_t)((g.Vh + 7) / 8) * 2;  // smallest block: 8 sites (RHS-in-lanes hop)
+  // most partial sums per RHS: one per warp of the RHS-in-lanes kernels; at 16 lanes a
+  // warp covers 2 sites, so both parities give up to Vh partials
+  const size_t nblk = (size_t)g.Vh + 64;
   if (e == cudaSuccess) e = cudaMalloc(&E->partials, sizeof(double) * nblk * n);
   if (e == cudaSuccess) e = cudaMalloc(&E->counters, sizeof(unsigned) * (n + 1));
-  if (e == cudaSuccess) e = cudaMallocHost(&E->h_pinned, sizeof(int) * (3 * n + 1));
+  if (e == cudaSuccess) e = cudaMallocHost(&E->h_pinned, sizeof(int) * (3 * n + 2));
+  if (e == cudaSuccess) e = cudaMalloc(&E->ru_iters, sizeof(int));
   if (e != cudaSuccess) {
     ctx->err = std::string("engine allocation: ") + cudaGetErrorString(e);
     wl_engine_destroy(E);
@@ -1278,6 +1330,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   cudaMemsetAsync(E->dbl, 0, sizeof(double) * kEngineDoubles * n, st);
   cudaMemsetAsync(E->ints, 0, sizeof(int) * (kEngineInts * n + 1), st);
   cudaMemsetAsync(E->counters, 0, sizeof(unsigned) * (n + 1), st);
+  cudaMemsetAsync(E->ru_iters, 0, sizeof(int), st);
   double* d = E->dbl;
   E->r2 = d + 0 * n; E->r2_new = d + 1 * n; E->pAp = d + 2 * n; E->r2_true = d + 3 * n;
   E->rmax2 = d + 4 * n; E->b2 = d + 5 * n; E->tol2 = d + 6 * n; E->beta = d + 7 * n;
@@ -1365,22 +1418,74 @@ static wl_status engine_admit_all(wl_engine* E, const void* b, const void* x0, c
 
 static wl_status build_graph(wl_engine* E, cudaStream_t st) {
   wl_ctx* ctx = E->ctx;
-  cudaGraph_t graph;
-  WL_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  const long long before = g_launches.load();
-  enqueue_iteration_any(E, st);
-  E->graph_kernels = g_launches.load() - before;
-  g_launches -= E->graph_kernels;  // captured, not launched
-  cudaError_t e = cudaStreamEndCapture(st, &graph);
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  cudaGraph_t graph = nullptr;
+  WL_CUDA(ctx, cudaGraphCreate(&graph, 0));
+  cudaError_t e = cudaGraphConditionalHandleCreate(&E->cond, graph, 0, cudaGraphCondAssignDefault);
   if (e != cudaSuccess) {
-    ctx->err = std::string("graph capture: ") + cudaGetErrorString(e);
+    cudaGraphDestroy(graph);
+    ctx->err = std::string("cudaGraphConditionalHandleCreate: ") + cudaGetErrorString(e);
     return WL_ERR_CUDA;
   }
-  e = cudaGraphInstantiate(&E->gexec, graph, 0);
+  E->use_cond = true;
+  const long long before = g_launches.load();
+  // part 1: sloppy operator, CG update, reliable-update decision
+  e = cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, mode);
+  if (e == cudaSuccess) {
+    enqueue_part(E, st, 1);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    std::vector<cudaGraphNode_t> dv;
+    e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
+    if (e == cudaSuccess) dv.assign(deps, deps + ndeps);
+    cudaGraph_t g1 = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(st, &g1);
+    if (e == cudaSuccess) e = e2;
+    const long long part13 = g_launches.load();
+    // part 2 in a conditional IF node
+    cudaGraphNode_t cond_node = nullptr;
+    if (e == cudaSuccess) {
+      // cudaGraphNodeParams has no default constructor (it holds a union): zeroed storage
+      alignas(cudaGraphNodeParams) unsigned char cpbuf[sizeof(cudaGraphNodeParams)];
+      std::memset(cpbuf, 0, sizeof(cpbuf));
+      cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cpbuf);
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = E->cond;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&cond_node, graph, dv.data(), dv.size(), &cp);
+      if (e == cudaSuccess) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, mode);
+        if (e == cudaSuccess) {
+          const long long b0 = g_launches.load();
+          enqueue_part(E, st, 2);
+          E->ru_body_kernels = g_launches.load() - b0;
+          cudaGraph_t gb = nullptr;
+          e = cudaStreamEndCapture(st, &gb);
+        }
+      }
+    }
+    // part 3 after the conditional node
+    if (e == cudaSuccess) {
+      const long long p3 = g_launches.load();
+      e = cudaStreamBeginCaptureToGraph(st, graph, &cond_node, nullptr, 1, mode);
+      if (e == cudaSuccess) {
+        enqueue_part(E, st, 3);
+        cudaGraph_t g3 = nullptr;
+        e = cudaStreamEndCapture(st, &g3);
+      }
+      E->graph_kernels = (part13 - before) + (g_launches.load() - p3);
+    }
+  }
+  g_launches = before;  // captured, not launched
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&E->gexec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) {
-    ctx->err = std::string("graph instantiate: ") + cudaGetErrorString(e);
+    E->use_cond = false;
     E->gexec = nullptr;
+    ctx->err = std::string("graph build: ") + cudaGetErrorString(e);
     return WL_ERR_CUDA;
   }
   E->graph_built = true;
@@ -1440,7 +1545,13 @@ extern "C" wl_status wl_engine_poll(wl_engine* E, int* status, int* n_active) {
   const int n = E->n;
   WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned, E->n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
   if (status) WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned + 1, E->status, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned + 1 + n, E->ru_iters, sizeof(int), cudaMemcpyDeviceToHost, st));
   WL_CUDA(ctx, cudaStreamSynchronize(st));
+  {  // kernels that ran inside the graph's conditional reliable-update body
+    const long long seen = E->h_pinned[1 + n];
+    g_launches += (seen - E->ru_iters_seen) * E->ru_body_kernels;
+    E->ru_iters_seen = seen;
+  }
   if (n_active) *n_active = E->h_pinned[0];
   if (status) std::memcpy(status, E->h_pinned + 1, sizeof(int) * n);
   return WL_OK;

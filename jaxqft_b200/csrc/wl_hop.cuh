@@ -168,12 +168,13 @@ WL_D void hop_dir(const Geom& g, const LF& links, const SF& src, int parity, con
   }
 }
 
-// Launch-wide reduction bookkeeping: per-block partial sums per RHS, then the
-// last block to finish (atomic ticket per blockIdx.y) sums the partials in a
-// fixed order and writes result[rhs].  Deterministic run to run.
+// Launch-wide reductions: every block writes one partial sum per RHS it
+// covers into partials[rhs][block]; reduce_finalize_kernel (launched right
+// after, one block per RHS) adds them in a fixed order.  Deterministic run to
+// run, no floating-point atomics and no per-block fences.
 struct Reduce {
   double* partials;   // [nrhs][nblk]
-  unsigned* counter;  // [gridDim.y], zero at allocation, self-resetting
+  unsigned* counter;  // unused (kept for layout stability)
   double* result;     // [nrhs]
 };
 
@@ -182,7 +183,6 @@ constexpr int kMaxRB = 16;  // RHS per block (BY * NR)
 template <int NR>
 WL_D void reduce_rhs(const double (&val)[NR], const Reduce& R, int nrhs, const int* mask) {
   __shared__ double sred[kMaxRB * 8];
-  __shared__ int s_last;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int lane = tx & 31, wx = tx >> 5, nwx = blockDim.x >> 5;
   const int RB = blockDim.y * NR;
@@ -204,27 +204,32 @@ WL_D void reduce_rhs(const double (&val)[NR], const Reduce& R, int nrhs, const i
     const int rhs = rbase + tid;
     if (rhs < nrhs) R.partials[(long long)rhs * nblk + blk] = x;
   }
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    unsigned t = atomicAdd(&R.counter[blockIdx.y], 1u);
-    s_last = (t == (unsigned)nblk - 1);
+}
+
+// result[rhs] = sum_b partials[rhs][b] in a fixed order, for RHS in `mask`:
+// one 512-thread block per RHS, four independent accumulators per thread.
+constexpr int kFinalizeThreads = 512;
+
+__global__ void __launch_bounds__(kFinalizeThreads) reduce_finalize_kernel(Reduce R, int nrhs, int nblk,
+                                                                            const int* mask) {
+  __shared__ double sm[32];
+  const int rhs = blockIdx.x;
+  if (rhs >= nrhs) return;
+  if (mask != nullptr && mask[rhs] == 0) return;  // uniform per block
+  const double* p = R.partials + (long long)rhs * nblk;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  const int step = 4 * kFinalizeThreads;
+  int b = threadIdx.x;
+  for (; b + 3 * kFinalizeThreads < nblk; b += step) {
+    a0 += p[b];
+    a1 += p[b + kFinalizeThreads];
+    a2 += p[b + 2 * kFinalizeThreads];
+    a3 += p[b + 3 * kFinalizeThreads];
   }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  const int nth = blockDim.x * blockDim.y;
-  for (int i = 0; i < RB; ++i) {
-    const int rhs = rbase + i;
-    if (rhs >= nrhs) break;  // uniform across the block
-    double v[1] = {0.0};
-    for (int b = tid; b < nblk; b += nth) v[0] += __ldcg(&R.partials[(long long)rhs * nblk + b]);
-    block_sum<1>(v, sred);
-    if (tid == 0 && (mask == nullptr || mask[rhs] != 0)) R.result[rhs] = v[0];
-    __syncthreads();
-  }
-  if (tid == 0) R.counter[blockIdx.y] = 0;
+  for (; b < nblk; b += kFinalizeThreads) a0 += p[b];
+  double v[1] = {(a0 + a1) + (a2 + a3)};
+  block_sum<1>(v, sm);
+  if (threadIdx.x == 0) R.result[rhs] = v[0];
 }
 
 // Generic launch parameters

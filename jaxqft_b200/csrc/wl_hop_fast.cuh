@@ -302,45 +302,20 @@ WL_D void lane_dir(const SF& src, const LinkSmem* Ls, const int* nbs, int rhs, f
   }
 }
 
+// Per-warp partial sums (no block barrier): after the xor-shuffles over the
+// sites of a warp, lanes 0..R-1 hold the warp's sum for RHS rbase + lane; warp
+// w of block b writes partials[rhs][b * 4 + w].
+constexpr int kLaneWarps = kLaneBlock / 32;
+
 template <int R>
-WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* mask) {
-  __shared__ double sw[kLaneBlock / 32][32];
-  __shared__ int s_last;
+WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* /*mask*/) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 #pragma unroll
   for (int off = R; off < 32; off <<= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-  if (lane < R) sw[warp][lane] = v;
-  __syncthreads();
-  const int nblk = gridDim.x * gridDim.z;
-  const int blk = blockIdx.z * gridDim.x + blockIdx.x;
-  const int rbase = blockIdx.y * R;
-  if (tid < R) {
-    double x = 0.0;
-#pragma unroll
-    for (int w = 0; w < kLaneBlock / 32; ++w) x += sw[w][tid];
-    if (rbase + tid < nrhs) Rd.partials[(long long)(rbase + tid) * nblk + blk] = x;
-  }
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    unsigned t = atomicAdd(&Rd.counter[blockIdx.y], 1u);
-    s_last = (t == (unsigned)nblk - 1);
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  double* sred = &sw[0][0];
-  for (int i = 0; i < R; ++i) {
-    const int rhs = rbase + i;
-    if (rhs >= nrhs) break;
-    double vv[1] = {0.0};
-    for (int b = tid; b < nblk; b += kLaneBlock) vv[0] += __ldcg(&Rd.partials[(long long)rhs * nblk + b]);
-    block_sum<1>(vv, sred);
-    if (tid == 0 && (mask == nullptr || mask[rhs] != 0)) Rd.result[rhs] = vv[0];
-    __syncthreads();
-  }
-  if (tid == 0) Rd.counter[blockIdx.y] = 0;
+  const int nblk = gridDim.x * gridDim.z * kLaneWarps;
+  const int blk = (blockIdx.z * gridDim.x + blockIdx.x) * kLaneWarps + warp;
+  const int rhs = blockIdx.y * R + lane;
+  if (lane < R && rhs < nrhs) Rd.partials[(long long)rhs * nblk + blk] = v;
 }
 
 template <bool DAG, int R, class LF, class SF, class EPI>

@@ -329,7 +329,14 @@ struct CGScalars {
 
 enum SlotStatus { ST_IDLE = 0, ST_RUNNING = 1, ST_CONVERGED = 2, ST_MAXITER = 3, ST_BREAKDOWN = 4, ST_NAN = 5 };
 
-__global__ void cg_decide_kernel(CGScalars S, int n) {
+// Decides which slots take a reliable update this iteration.  In a CUDA graph
+// with a conditional node (`use_cond`), also switches the node's body (the FP64
+// true-residual kernels) on only when at least one slot needs it, and counts
+// such iterations in *ru_iters.
+__global__ void cg_decide_kernel(CGScalars S, int n, int use_cond, cudaGraphConditionalHandle cond, int* ru_iters) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
   for (int s = threadIdx.x; s < n; s += blockDim.x) {
     S.ru[s] = 0;
     if (!S.active[s]) continue;
@@ -347,6 +354,12 @@ __global__ void cg_decide_kernel(CGScalars S, int n) {
     }
     const bool trig = (r2n < S.delta2 * S.rmax2[s]) || (r2n <= S.tol2[s] * S.b2[s]) || (S.iters[s] + 1 >= S.maxiter[s]);
     S.ru[s] = trig ? 1 : 0;
+    if (trig) atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (any && ru_iters) *ru_iters += 1;
+    if (use_cond) cudaGraphSetConditional(cond, any ? 1u : 0u);
   }
 }
 
