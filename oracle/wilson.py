@@ -411,6 +411,40 @@ def evolve_q(dt, P, U):
 
 
 # --------------------------------------------------------------------------
+# HMC molecular dynamics (core/integrators.py:46-58, core/update.py:51-78)
+# --------------------------------------------------------------------------
+def total_force(U, phi, mass, bc, beta, tol, eo=False):
+    """Gauge force + analytic Nf=2 pseudofermion force (monomial force_analytic,
+    su3_wilson_nf2.py:374-389 and 566-579)."""
+    F = gauge_force(U, beta)
+    if eo:
+        xe, _ = solve_eop_even_normal(U, phi, mass, bc, tol, 10000)
+        ye = schur_even(U, xe, mass, bc, normalized=True)
+        return F + eop_force_from_solution(U, xe, ye, mass, bc)
+    x, _ = solve_normal(U, phi, mass, bc, tol, 10000)
+    return F + force_from_solution(U, x, apply_D(U, x, mass, bc), bc)
+
+
+def hamiltonian(U, P, phi, mass, bc, beta, tol, eo=False):
+    if eo:
+        sf = eop_pseudofermion_action(U, phi, mass, bc, tol, 10000)
+    else:
+        sf = pseudofermion_action(U, phi, mass, bc, tol, 10000)
+    return kinetic(P) + gauge_action(U, beta) + sf
+
+
+def minnorm2(P, U, force, nmd, tau, lam=0.1931833275037836):
+    dt = tau / nmd
+    for _ in range(nmd):
+        P = P + dt * lam * force(U)
+        U = evolve_q(0.5 * dt, P, U)
+        P = P + dt * (1.0 - 2.0 * lam) * force(U)
+        U = evolve_q(0.5 * dt, P, U)
+        P = P + dt * lam * force(U)
+    return P, U
+
+
+# --------------------------------------------------------------------------
 # seeded inputs
 # --------------------------------------------------------------------------
 def hot_links(rng, shape, batch, scale):
