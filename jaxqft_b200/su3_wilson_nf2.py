@@ -139,9 +139,7 @@ class WilsonNf2PseudofermionMonomial(_PFBase):
     def action(self, q):
         if self.phi is None:
             self.refresh(q, traj_length=1.0)
-        x0 = self._guess()
-        x = self.model.solve_normal(q, self.phi) if x0 is None else self.model.solve_normal_with_guess(q, self.phi, x0)
-        self._remember(x)
+        x = self.model.solve_normal(q, self.phi, tol=self.model.action_cg_tol)
         return torch.stack([_vdot(self.phi[b], x[b]).real for b in range(x.shape[0])])
 
     def force_analytic(self, q, phi):
@@ -179,10 +177,7 @@ class WilsonNf2EOPreconditionedMonomial(_PFBase):
     def action(self, q):
         if self.phi is None:
             self.refresh(q, traj_length=1.0)
-        m = self.model
-        x0 = self._guess()
-        x = m.solve_eop_even_normal(q, self.phi) if x0 is None else m.solve_eop_even_normal_with_guess(q, self.phi, x0)
-        self._remember(x)
+        x = self.model.solve_eop_even_normal(q, self.phi, tol=self.model.action_cg_tol)
         return torch.stack([_vdot(self.phi[b], x[b]).real for b in range(x.shape[0])])
 
     def force_analytic(self, q, phi):
@@ -229,6 +224,7 @@ class SU3WilsonNf2(SU3YangMills):
     jit_solvers: bool = True
     solver_precision: str = "double"
     reliable_delta: float = 0.1
+    action_cg_tol: Optional[float] = None  # tighter tolerance for the Metropolis action solves
     requires_trajectory_refresh: bool = field(default=False, init=False)
     _skip_next_trajectory_refresh: bool = field(default=False, init=False, repr=False)
 
@@ -438,14 +434,15 @@ class SU3WilsonNf2(SU3YangMills):
         return self.apply_Ddag(U, self.random_fermion())
 
     # ------------------------------------------------------------------ solves (:1243-1454)
-    def _solve(self, op: str, U, rhs, x0=None):
+    def _solve(self, op: str, U, rhs, x0=None, tol: Optional[float] = None):
         gauges = self._gauges_for(U)
+        tol = self.cg_tol if tol is None else float(tol)
         rhs = self._as_tensor(rhs)
         x0 = None if x0 is None else self._as_tensor(x0)
         out = torch.empty_like(rhs)
         stats = []
         for b in range(rhs.shape[0]):
-            x, st = self.ctx.solve(gauges[b], rhs[b], self.mass, op=op, tol=self.cg_tol, maxiter=self.cg_maxiter,
+            x, st = self.ctx.solve(gauges[b], rhs[b], self.mass, op=op, tol=tol, maxiter=self.cg_maxiter,
                                    inner=self.solver_precision, delta=self.reliable_delta,
                                    x0=None if x0 is None else x0[b])
             out[b] = x
@@ -454,17 +451,17 @@ class SU3WilsonNf2(SU3YangMills):
         if any(s["status"] == L.SLOT_NAN for s in stats):
             raise L.WilsonError(L.WL_ERR_NAN, "solver produced a non-finite residual")
         if any(s["status"] != L.SLOT_CONVERGED for s in stats):
-            warnings.warn(f"CG did not reach tol {self.cg_tol} within {self.cg_maxiter} iterations", RuntimeWarning)
+            warnings.warn(f"CG did not reach tol {tol} within {self.cg_maxiter} iterations", RuntimeWarning)
         return self._out(out)
 
-    def solve_normal(self, U, phi):
-        return self._solve("normal", U, phi)
+    def solve_normal(self, U, phi, tol: Optional[float] = None):
+        return self._solve("normal", U, phi, tol=tol)
 
     def solve_normal_with_guess(self, U, phi, x0):
         return self._solve("normal", U, phi, x0)
 
-    def solve_eop_even_normal(self, U, rhs):
-        return self._solve("eo_normal", U, self._project_even(rhs))
+    def solve_eop_even_normal(self, U, rhs, tol: Optional[float] = None):
+        return self._solve("eo_normal", U, self._project_even(rhs), tol=tol)
 
     def solve_eop_even_normal_with_guess(self, U, rhs, x0):
         return self._solve("eo_normal", U, self._project_even(rhs), self._project_even(x0))

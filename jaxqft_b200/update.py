@@ -4,7 +4,7 @@
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import List
+from typing import Callable, List, Optional
 
 import numpy as np
 import torch
@@ -18,6 +18,7 @@ class HMC:
     seed: int = 0
     AcceptReject: List[float] = field(default_factory=list)
     history: List[dict] = field(default_factory=list)
+    uniform: Optional[Callable] = None  # shape -> uniforms in [0,1); default: seeded torch RNG
 
     def __post_init__(self):
         dev = getattr(self.T, "device", None)
@@ -50,12 +51,16 @@ class HMC:
             Hf = self.T.kinetic(p) + self.T.action(q_prop)
             dH = (Hf - H0).to(torch.float64)
             acc_prob = torch.where(dH < 0, torch.ones_like(dH), torch.exp(-dH))
-            R = torch.rand(acc_prob.shape, generator=self.generator, device=acc_prob.device, dtype=torch.float64)
+            if self.uniform is not None:
+                R = torch.as_tensor(self.uniform(acc_prob.shape), dtype=torch.float64, device=acc_prob.device)
+            else:
+                R = torch.rand(acc_prob.shape, generator=self.generator, device=acc_prob.device, dtype=torch.float64)
             acc = R < acc_prob
             self.AcceptReject.extend(acc.to(torch.float64).cpu().tolist())
             shape = [q.shape[0]] + [1] * (q.ndim - 1)
             q = torch.where(acc.reshape(shape), q_prop, q0)
-            self.history.append({"dH": dH.cpu().tolist(), "accepted": acc.cpu().tolist()})
+            self.history.append({"dH": dH.cpu().tolist(), "accepted": acc.cpu().tolist(),
+                                 "H0": H0.cpu().tolist()})
             if self.verbose:
                 print(" HMC:", k, " dH=", dH.cpu().tolist(), " A/R=", acc.cpu().tolist(),
                       " Pacc=", float(acc.to(torch.float64).mean()))
