@@ -268,6 +268,12 @@ def run_ours(args):
         e2e = {"value": world * NRHS / tmax, "unit": "solves/s", "h2d_bytes_per_step": int(nbytes),
                "d2h_bytes_per_step": int(nbytes)}
 
+    # ---- serving: Poisson stream of propagator requests, continuous batching
+    serve = None
+    if args.serve_seconds > 0:
+        eng.close()
+        serve = run_serving(args, dev)
+
     # ---- CPU baseline (rank 0, N=1): C restatement of the reference's FP64 CG
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -299,15 +305,46 @@ def run_ours(args):
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": hop_bytes,
                          "ms_per_launch": hop_ms, "traffic": traffic},
             "e2e": e2e,
+            "serve": serve,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    eng.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+SERVE_VOLUMES = [(8, 8, 8, 8), (12, 12, 12, 24), (16, 16, 16, 32), (24, 24, 24, 48)]
+
+
+def run_serving(args, dev):
+    """Serving workload: Poisson arrivals (mean 50/s) over `serve_seconds`,
+    volume uniform over {8^4, 12^3x24, 16^3x32, 24^3x48}, kappa uniform in
+    [0.120, 0.135], 1-12 point or Gaussian RHS each, on 4 resident gauge fields
+    per volume (exp(i*0.2*H), seeds 0-3), admission by HBM budget, true residual
+    1e-10.  Latency includes queueing (arrival to last RHS converged)."""
+    from jaxqft_b200.serving import PropagatorServer, poisson_requests, summarize
+
+    server = PropagatorServer(SERVE_VOLUMES, gauge_seeds=(0, 1, 2, 3), nslots=16, inner="half", tol=TOL,
+                              device=dev)
+    # warm-up: one small request per volume (engine creation, graph capture, autotune)
+    warm = poisson_requests(1000.0, 0.02, SERVE_VOLUMES, seed=99)[:4]
+    for i, r in enumerate(warm):
+        r.volume, r.t_arrive = SERVE_VOLUMES[i % 4], 0.0
+    server.run(warm)
+    server.done = []
+    reqs = poisson_requests(args.serve_rate, args.serve_seconds, SERVE_VOLUMES, seed=1)
+    t0 = time.perf_counter()
+    done = server.run(reqs)
+    wall = time.perf_counter() - t0
+    s = summarize(done, wall)
+    s.update({"rate_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,
+              "volumes": ["x".join(map(str, v)) for v in SERVE_VOLUMES], "gauge_fields_per_volume": 4,
+              "hbm_budget_GB": server.hbm_budget / 1e9, "peak_engine_GB": server.peak_engine_bytes / 1e9})
+    server.close()
+    return s
 
 
 # --------------------------------------------------------------------------- CPU legs
@@ -418,6 +455,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=4.0, help="serving leg: seconds of Poisson arrivals (0: off)")
+    ap.add_argument("--serve-rate", type=float, default=50.0, help="serving leg: mean requests per second")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--fp64-all", action="store_true", help="time plain FP64 CG on all 16 RHS (default 4)")
     ap.add_argument("--profile-iters", type=int, default=0,

@@ -1,0 +1,264 @@
+"""Continuous-batching propagator-solve server on one B200.
+
+Requests ask for Wilson propagator columns: for each of their RHS (point
+sources at site 0 or Gaussian spinors) solve the even-odd normal system
+(M^dag M) x = M^dag eta on one of the resident gauge fields, at the request's
+own kappa, to an FP64 true residual <= tol.  This is the solve pattern of
+jaxqft/core/measurements.py:277-372 (sources passed through the adjoint, then
+a normal-equation CG), batched across requests.
+
+* Gauge fields stay resident in HBM (per volume, one per seed).
+* One solver engine (``wl_engine``) per (volume, gauge field) holds a fixed set
+  of RHS slots with per-slot kappa/tolerance; a request is admitted into free
+  slots while other slots of the same engine are mid-solve, and its slots are
+  retired (and freed) as they converge -- continuous batching at RHS level.
+* Engines are created on demand while the sum of their device footprints
+  (``wl_engine_bytes``) stays under the HBM budget; requests that do not fit
+  wait in a FIFO queue.  Each engine runs on its own CUDA stream, so work for
+  different volumes / gauge fields overlaps on the device.
+* Latency = completion - arrival (queueing included), measured on the host
+  clock; each response's solution stays in device memory.
+"""
+
+from __future__ import annotations
+
+import collections
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import lib as L
+
+
+@dataclass
+class Request:
+    rid: int
+    volume: Tuple[int, ...]
+    gauge: int
+    kappa: float
+    nrhs: int
+    kind: str  # "point" | "gaussian"
+    t_arrive: float
+    seed: int = 0
+    t_admit: Optional[float] = None
+    t_done: Optional[float] = None
+    slots: List[int] = field(default_factory=list)
+    eta: Optional[torch.Tensor] = None
+    b: Optional[torch.Tensor] = None
+    x: Optional[torch.Tensor] = None
+    stats: List[dict] = field(default_factory=list)
+    pending: int = 0
+
+    @property
+    def mass(self) -> float:
+        return 1.0 / (2.0 * self.kappa) - 4.0
+
+    @property
+    def latency_ms(self) -> float:
+        return (self.t_done - self.t_arrive) * 1e3
+
+
+def make_sources(req: Request, device) -> torch.Tensor:
+    """Raw sources eta for a request: point sources delta(x,0) delta(s,c; k)
+    for k = 0..nrhs-1 (spin x colour), or complex Gaussians with E|z|^2 = 1."""
+    eta = torch.zeros((req.nrhs, *req.volume, 4, 3), dtype=torch.complex128, device=device)
+    if req.kind == "point":
+        for k in range(req.nrhs):
+            eta[k, 0, 0, 0, 0, (k % 12) // 3, k % 3] = 1.0
+    else:
+        g = torch.Generator(device=device)
+        g.manual_seed(int(req.seed))
+        shp = eta.shape
+        eta = torch.complex(torch.randn(shp, generator=g, device=device, dtype=torch.float64),
+                            torch.randn(shp, generator=g, device=device, dtype=torch.float64)) / math.sqrt(2.0)
+    return eta
+
+
+def even_mask(volume, device) -> torch.Tensor:
+    par = torch.zeros(volume, dtype=torch.int64, device=device)
+    for ax, n in enumerate(volume):
+        shp = [1] * 4
+        shp[ax] = n
+        par = par + torch.arange(n, device=device).reshape(shp)
+    return (par % 2 == 0).to(torch.complex128)[..., None, None]
+
+
+class _Slotted:
+    """An engine plus slot bookkeeping."""
+
+    def __init__(self, engine: L.Engine, nslots: int, nbytes: int):
+        self.engine = engine
+        self.nslots = nslots
+        self.nbytes = nbytes
+        self.owner: Dict[int, Tuple[Request, int]] = {}  # slot -> (request, rhs index)
+
+    @property
+    def free(self) -> int:
+        return self.nslots - len(self.owner)
+
+    def free_slots(self, k: int) -> List[int]:
+        return [s for s in range(self.nslots) if s not in self.owner][:k]
+
+
+class PropagatorServer:
+    def __init__(self, volumes: Sequence[Tuple[int, ...]], gauge_seeds: Sequence[int] = (0, 1, 2, 3),
+                 link_scale: float = 0.2, nslots: int = 16, inner: str = "half", tol: float = 1e-10,
+                 maxiter: int = 4000, hbm_budget_bytes: Optional[int] = None, iters_per_poll: int = 8,
+                 device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("the serving loop requires a CUDA device")
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.nslots, self.inner, self.tol, self.maxiter = int(nslots), inner, float(tol), int(maxiter)
+        self.iters_per_poll = int(iters_per_poll)
+        free, total = torch.cuda.mem_get_info(self.device)
+        self.hbm_budget = int(hbm_budget_bytes) if hbm_budget_bytes is not None else int(0.6 * free)
+        self.ctx: Dict[Tuple[int, ...], L.WilsonContext] = {}
+        self.gauges: Dict[Tuple[Tuple[int, ...], int], L.Gauge] = {}
+        self.resident_bytes = 0
+        for vol in volumes:
+            vol = tuple(int(v) for v in vol)
+            self.ctx[vol] = L.WilsonContext(vol, bc=(1, 1, 1, -1), device=self.device)
+            for seed in gauge_seeds:
+                U = self._hot_links(vol, link_scale, seed)
+                self.gauges[(vol, int(seed))] = self.ctx[vol].gauge(U)
+                self.resident_bytes += int(np.prod(vol)) * 4 * 9 * 16 * 2 + int(np.prod(vol)) * 4 * 9 * 16
+                del U
+        self.engines: Dict[Tuple[Tuple[int, ...], int], _Slotted] = {}
+        self.engine_bytes = 0
+        self.peak_engine_bytes = 0
+        self.queue: collections.deque = collections.deque()
+        self.done: List[Request] = []
+
+    def _hot_links(self, vol, scale, seed):
+        g = torch.Generator(device=self.device)
+        g.manual_seed(int(seed))
+        shp = (4, *vol, 3, 3)
+        a = scale * torch.complex(torch.randn(shp, generator=g, device=self.device, dtype=torch.float64),
+                                  torch.randn(shp, generator=g, device=self.device, dtype=torch.float64))
+        y = 0.5 * (a - a.conj().transpose(-1, -2))
+        tr = torch.diagonal(y, dim1=-2, dim2=-1).sum(-1) / 3.0
+        y = y - tr[..., None, None] * torch.eye(3, dtype=y.dtype, device=self.device)
+        return torch.linalg.matrix_exp(y)
+
+    # ------------------------------------------------------------------ admission
+    def _engine_for(self, req: Request) -> Optional[_Slotted]:
+        key = (req.volume, req.gauge)
+        if key in self.engines:
+            return self.engines[key]
+        ctx = self.ctx[req.volume]
+        nbytes = ctx.engine_bytes("eo_normal", self.inner, self.nslots)
+        if self.engine_bytes + nbytes > self.hbm_budget:
+            # release an idle engine to make room, if any
+            for k, e in list(self.engines.items()):
+                if not e.owner:
+                    e.engine.close()
+                    self.engine_bytes -= e.nbytes
+                    del self.engines[k]
+                    if self.engine_bytes + nbytes <= self.hbm_budget:
+                        break
+        if self.engine_bytes + nbytes > self.hbm_budget:
+            return None
+        eng = L.Engine(ctx, self.gauges[key], self.nslots, op="eo_normal", inner=self.inner, tol=self.tol,
+                       maxiter=self.maxiter)
+        se = _Slotted(eng, self.nslots, nbytes)
+        self.engines[key] = se
+        self.engine_bytes += nbytes
+        self.peak_engine_bytes = max(self.peak_engine_bytes, self.engine_bytes)
+        return se
+
+    def _admit(self, req: Request, se: _Slotted, now: float) -> None:
+        ctx, gauge = self.ctx[req.volume], self.gauges[(req.volume, req.gauge)]
+        eta = make_sources(req, self.device) * even_mask(req.volume, self.device)
+        # b = M^dag eta_e on the engine's own stream ordering (ctx stream, then engine waits)
+        req.b = ctx.apply("SCHUR_E_DAG", gauge, req.mass, eta, normalized=True)
+        req.slots = se.free_slots(req.nrhs)
+        for i, s in enumerate(req.slots):
+            se.owner[s] = (req, i)
+        req.x = torch.empty_like(req.b)
+        req.stats = [None] * req.nrhs
+        req.pending = req.nrhs
+        se.engine.admit(req.slots, req.b, np.full(req.nrhs, req.mass), tols=np.full(req.nrhs, self.tol))
+        req.t_admit = now
+
+    def _try_admit(self, now: float) -> None:
+        waiting = collections.deque()
+        while self.queue:
+            req = self.queue.popleft()
+            if req.nrhs > self.nslots:
+                raise ValueError(f"request {req.rid}: {req.nrhs} RHS exceed the {self.nslots} slots of an engine")
+            se = self._engine_for(req)
+            if se is not None and se.free >= req.nrhs:
+                self._admit(req, se, now)
+            else:
+                waiting.append(req)
+        self.queue = waiting
+
+    # ------------------------------------------------------------------ main loop
+    def run(self, requests: Sequence[Request], time_fn=time.perf_counter) -> List[Request]:
+        """Serve `requests` (arrival times in seconds from the start)."""
+        pending = collections.deque(sorted(requests, key=lambda r: r.t_arrive))
+        t0 = time_fn()
+        while pending or self.queue or any(e.owner for e in self.engines.values()):
+            now = time_fn() - t0
+            while pending and pending[0].t_arrive <= now:
+                self.queue.append(pending.popleft())
+            if self.queue:
+                self._try_admit(now)
+            busy = [e for e in self.engines.values() if e.owner]
+            if not busy:
+                if pending:
+                    time.sleep(max(0.0, min(pending[0].t_arrive - (time_fn() - t0), 0.01)))
+                continue
+            for e in busy:  # queue iterations on every engine's stream before any sync
+                e.engine.step(self.iters_per_poll)
+            for e in busy:
+                st, _ = e.engine.poll()
+                for s in list(e.owner):
+                    if st[s] >= L.SLOT_CONVERGED:
+                        req, i = e.owner.pop(s)
+                        _, info = e.engine.retire(s, out=req.x[i])
+                        req.stats[i] = info
+                        req.pending -= 1
+                        if req.pending == 0:
+                            req.t_done = time_fn() - t0
+                            self.done.append(req)
+        torch.cuda.synchronize(self.device)
+        return self.done
+
+    def close(self):
+        for e in self.engines.values():
+            e.engine.close()
+        self.engines.clear()
+
+
+def poisson_requests(rate: float, duration: float, volumes, kappa_range=(0.120, 0.135), max_rhs: int = 12,
+                     ngauge: int = 4, seed: int = 0) -> List[Request]:
+    """Poisson arrivals (mean `rate` per second) over `duration` seconds with
+    volume, kappa, RHS count and source kind drawn uniformly."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        vol = tuple(volumes[rng.integers(len(volumes))])
+        out.append(Request(rid=len(out), volume=vol, gauge=int(rng.integers(ngauge)),
+                           kappa=float(rng.uniform(*kappa_range)), nrhs=int(rng.integers(1, max_rhs + 1)),
+                           kind="point" if rng.random() < 0.5 else "gaussian", t_arrive=t,
+                           seed=int(rng.integers(1 << 30))))
+    return out
+
+
+def summarize(done: Sequence[Request], wall: float) -> dict:
+    lat = np.array([r.latency_ms for r in done])
+    nsol = sum(r.nrhs for r in done)
+    res = max((s["true_res"] for r in done for s in r.stats), default=0.0)
+    conv = all(s["status"] == L.SLOT_CONVERGED for r in done for s in r.stats)
+    return {"requests": len(done), "solves": nsol, "wall_s": wall, "solves_per_s": nsol / wall if wall > 0 else 0.0,
+            "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+            "mean_ms": float(lat.mean()) if len(lat) else None, "max_true_res": res, "all_converged": conv}
