@@ -172,7 +172,7 @@ def run_ours(args):
     b = ctx.apply("SCHUR_E_DAG", gauge, MASS, eta * even_mask(torch, dev), normalized=True)
     torch.cuda.synchronize()
 
-    eng = L.Engine(ctx, gauge, NRHS, op="eo_normal", inner="half", tol=TOL, maxiter=4000, delta=0.1)
+    eng = L.Engine(ctx, gauge, NRHS, op="eo_normal", inner=args.inner, tol=TOL, maxiter=4000, delta=args.delta)
     estream = eng.stream
     x = torch.empty_like(b)
     slots = np.arange(NRHS)
@@ -291,14 +291,16 @@ def run_ours(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32 arithmetic on f16 storage + f64 reliable updates",
+            "dtype": ("f32 arithmetic on f16 storage" if args.inner == "half" else "f32" if args.inner == "single"
+                      else "f64") + " + f64 reliable updates",
             "data": "synthetic (seeded links exp(i*0.2*H), point + Gaussian sources)",
             "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, SHAPE)), "kappa": KAPPA,
                        "nrhs": NRHS, "tol": TOL, "parallelism": f"replicas x{world} (independent solves)",
                        "l2": "working set > 126 MB L2 (no flush needed)"},
             "fp64_cg": {"solves_per_s": fp64_sps * world, "iters": it64, "note": "plain FP64 CG, one RHS at a time"},
             "speedup_vs_fp64": value / (fp64_sps * world),
-            "solve": {"iters_min": min(iters), "iters_max": max(iters), "max_true_res": res, "all_converged": conv,
+            "solve": {"inner": args.inner, "delta": args.delta, "iters_min": min(iters), "iters_max": max(iters),
+                      "max_true_res": res, "all_converged": conv,
                       "reliable_updates_max": max(s["reliable_updates"] for s in all_stats[-1])},
             "roofline": {"bound": "hbm", "kernel": "hop (FP16 storage, 12-real links, 16 RHS, EO parity)",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
@@ -455,6 +457,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--delta", type=float, default=0.1, help="reliable-update threshold of the mixed solver")
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="serving leg: seconds of Poisson arrivals (0: off)")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="serving leg: mean requests per second")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
