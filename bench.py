@@ -148,6 +148,21 @@ def even_mask(torch, device):
 
 
 # --------------------------------------------------------------------------- our arm
+def aggregate_over_ranks(t_local: float, units_per_rank: int, dist=None, device=None):
+    """Whole-job throughput of independent replicas: every rank solved
+    `units_per_rank` systems in `t_local` seconds (device time); the job time
+    is the max over ranks and the value is world * units / that time."""
+    import torch
+
+    world = 1 if dist is None else dist.get_world_size()
+    t_max = float(t_local)
+    if dist is not None:
+        tt = torch.tensor([t_max], device=device, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    return t_max, world * units_per_rank / t_max
+
+
 def run_ours(args):
     import torch
 
@@ -212,13 +227,7 @@ def run_ours(args):
             all_stats.append(stats)
     torch.cuda.synchronize()
     launches = L.kernel_launches() - launches0
-    t_step = float(np.mean(times))
-    t_max = t_step
-    if dist is not None:
-        tt = torch.tensor([t_step], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    value = world * NRHS / t_max
+    t_max, value = aggregate_over_ranks(float(np.mean(times)), NRHS, dist, dev)
     iters = [s["iters"] for s in all_stats[-1]]
     res = max(s["true_res"] for st in all_stats for s in st)
     conv = all(s["status"] == 2 for st in all_stats for s in st)
@@ -259,13 +268,9 @@ def run_ours(args):
         for _ in range(max(1, min(args.steps, 3))):
             t, st = timed(e2e_once, cur)
             te.append(t)
-        tmax = float(np.mean(te))
-        if dist is not None:
-            tt = torch.tensor([tmax], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            tmax = float(tt.item())
+        _, e2e_value = aggregate_over_ranks(float(np.mean(te)), NRHS, dist, dev)
         nbytes = b_host.numel() * b_host.element_size()
-        e2e = {"value": world * NRHS / tmax, "unit": "solves/s", "h2d_bytes_per_step": int(nbytes),
+        e2e = {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(nbytes),
                "d2h_bytes_per_step": int(nbytes)}
 
     # ---- serving: Poisson stream of propagator requests, continuous batching

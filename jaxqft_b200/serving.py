@@ -226,7 +226,8 @@ class PropagatorServer:
                         if req.pending == 0:
                             req.t_done = time_fn() - t0
                             self.done.append(req)
-        torch.cuda.synchronize(self.device)
+        if self.device.type == "cuda":
+            torch.cuda.synchronize(self.device)
         return self.done
 
     def close(self):
