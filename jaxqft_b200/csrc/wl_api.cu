@@ -107,18 +107,18 @@ static SpinorField<P> sf(const IField& f, int par) {
   const long long ch = chunks_of(P), vh = f.vh, n = f.nrhs;
   if (!f.rhs_inner) {
     s.ptr = reinterpret_cast<Ptr>(f.data) + par * ch * vh;
-    s.rstride = ch * vh * f.npar;
-    s.kstride = vh;
+    s.rstride = (unsigned)(ch * vh * f.npar);
+    s.kstride = (unsigned)vh;
     s.cstride = 1;
-    s.nrstride = vh;
+    s.nrstride = (unsigned)vh;
     s.ncstride = 1;
   } else {
     s.ptr = reinterpret_cast<Ptr>(f.data) + par * ch * vh * n;
     s.rstride = 1;
-    s.kstride = vh * n;
-    s.cstride = n;
+    s.kstride = (unsigned)(vh * n);
+    s.cstride = (unsigned)n;
     s.nrstride = 1;
-    s.ncstride = n;
+    s.ncstride = (unsigned)n;
   }
   s.norm = f.norm ? f.norm + par * n * vh : nullptr;
   return s;
@@ -136,6 +136,8 @@ static wl_status alloc_field(wl_ctx* ctx, IField& f, int prec, int vh, int nrhs,
   f.nrhs = nrhs;
   f.npar = npar;
   f.rhs_inner = rhs_inner;
+  if ((unsigned long long)chunks_of(prec) * vh * npar * nrhs >= (1ull << 32))
+    WL_FAIL(ctx, WL_ERR_ARG, "field of 2^32 or more 16-byte chunks (32-bit offsets): use fewer RHS per engine");
   size_t data = (size_t)chunks_of(prec) * 16 * vh * npar * nrhs;
   size_t nb = data + (prec == P_HALF ? (size_t)vh * npar * nrhs * sizeof(float) : 0);
   WL_CUDA(ctx, cudaMalloc(&f.data, nb));
@@ -301,6 +303,9 @@ extern "C" wl_status wl_ctx_create(const wl_geometry* geom, int device, wl_ctx**
   g.strideRow[0] = g.L[1] * g.L[2];
   g.strideRow[1] = g.L[2];
   g.strideRow[2] = 1;
+  g.fd_lth = make_fastdiv((unsigned)g.Lth);
+  g.fd_l2 = make_fastdiv((unsigned)g.L[2]);
+  g.fd_l1 = make_fastdiv((unsigned)g.L[1]);
   for (int mu = 0; mu < 4; ++mu) {
     g.ph_re[mu] = geom->bc_re[mu];
     g.ph_im[mu] = geom->bc_im[mu];

@@ -62,6 +62,27 @@ template <typename T> WL_D void zero(Spinor<T>& s) {
 }
 
 // ---------------------------------------------------------------- geometry
+// Division by a run-time invariant d by multiply-high and shift (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", PLDI
+// 1994): with l = ceil(log2 d) and the round-up multiplier
+// m = ceil(2^(31+l) / d) < 2^32, floor(n/d) = floor(n m / 2^(31+l)) for every
+// 0 <= n < 2^31, i.e. __umulhi(n, m) >> (l-1).  d == 1 is flagged by m == 0.
+struct FastDiv {
+  unsigned d, mul, shr;
+};
+
+inline FastDiv make_fastdiv(unsigned d) {
+  FastDiv f{d, 0u, 0u};
+  if (d <= 1) return f;
+  unsigned l = 0;
+  while ((1ull << l) < d) ++l;
+  f.mul = (unsigned)(((1ull << (31 + l)) + d - 1) / d);
+  f.shr = l - 1;
+  return f;
+}
+
+WL_D unsigned fdiv(const FastDiv& f, unsigned n) { return f.mul ? (__umulhi(n, f.mul) >> f.shr) : n; }
+
 struct Geom {
   int L[4];      // Lx, Ly, Lz, Lt
   int Lth;       // Lt / 2
@@ -70,6 +91,7 @@ struct Geom {
   int strideRow[3];  // row stride of x, y, z in units of rows: Ly*Lz, Lz, 1
   double ph_re[4], ph_im[4];  // boundary phase per direction
   int ph_on[4];               // phase != 1
+  FastDiv fd_lth, fd_l2, fd_l1;  // divisions by Lt/2, Lz, Ly in the compact-index decomposition
 };
 
 struct Site {
@@ -81,13 +103,13 @@ struct Site {
 WL_D Site site_from_compact(const Geom& g, int parity, int c) {
   Site s;
   s.c = c;
-  int th = c % g.Lth;
-  int row = c / g.Lth;
+  const int row = (int)fdiv(g.fd_lth, (unsigned)c);
+  const int th = c - row * g.Lth;
   s.row = row;
-  s.x[2] = row % g.L[2];
-  int r2 = row / g.L[2];
-  s.x[1] = r2 % g.L[1];
-  s.x[0] = r2 / g.L[1];
+  const int r2 = (int)fdiv(g.fd_l2, (unsigned)row);
+  s.x[2] = row - r2 * g.L[2];
+  s.x[0] = (int)fdiv(g.fd_l1, (unsigned)r2);
+  s.x[1] = r2 - s.x[0] * g.L[1];
   s.x[3] = 2 * th + ((parity + s.x[0] + s.x[1] + s.x[2]) & 1);
   return s;
 }
@@ -134,12 +156,14 @@ template <int P> struct SpinorField;
 //   RHS-innermost [k][Vh][nrhs]: rstride = 1, kstride = Vh*nrhs, cstride = nrhs
 // The first coalesces when consecutive lanes are consecutive sites, the second
 // when consecutive lanes are consecutive RHS of one site.  FP16 norms use
-// norm[rhs*nrstride + c*ncstride] likewise.
+// norm[rhs*nrstride + c*ncstride] likewise.  Offsets are 32-bit unsigned (the
+// allocator refuses fields of 2^32 chunks or more), which keeps the address
+// arithmetic of the stencil loads to one multiply-add per access.
 struct Strides {
-  long long rstride, kstride, cstride;
-  long long nrstride, ncstride;
-  WL_D long long at(int rhs, int k, long long c) const { return rhs * rstride + k * kstride + c * cstride; }
-  WL_D long long nat(int rhs, long long c) const { return rhs * nrstride + c * ncstride; }
+  unsigned rstride, kstride, cstride;
+  unsigned nrstride, ncstride;
+  WL_D unsigned at(int rhs, int k, unsigned c) const { return rhs * rstride + k * kstride + c * cstride; }
+  WL_D unsigned nat(int rhs, unsigned c) const { return rhs * nrstride + c * ncstride; }
 };
 
 template <> struct SpinorField<P_DOUBLE> : Strides {

@@ -338,10 +338,14 @@ __global__ void __launch_bounds__(kLaneBlock) hop_lanes_kernel(HopArgs<LF, SF, E
       // the forward hop from x_mu = L-1 uses ph*U; the backward hop into
       // x_mu = 0 uses (ph*U)^dag, i.e. the same phase-multiplied link
       const bool ph = A.g.ph_on[mu] && (dir == 0 ? (s.x[mu] == A.g.L[mu] - 1) : (s.x[mu] == 0));
-      const float pr = ph ? (float)A.g.ph_re[mu] : 1.f, pi = ph ? (float)A.g.ph_im[mu] : 0.f;
+      if (ph) {
+        const cplx<float> w{(float)A.g.ph_re[mu], (float)A.g.ph_im[mu]};
+#pragma unroll
+        for (int k = 0; k < 9; ++k) u.m[k / 3][k % 3] = u.m[k / 3][k % 3] * w;
+      }
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
-        const cplx<float> v = u.m[k / 3][k % 3] * cplx<float>{pr, pi};
+        const cplx<float> v = u.m[k / 3][k % 3];
         sm.link[sl].l[q].p[k] = make_float4(v.re, v.re, -v.im, v.im);
       }
       sm.nb[sl][q] = nb;
