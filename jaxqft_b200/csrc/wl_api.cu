@@ -204,8 +204,10 @@ template <bool DAG, class IDX, class LF, class SF, class EPI>
 static void launch_hop(const Tune& t, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st) {
   launch_hop_impl<DAG, IDX>(t, a, npar, st);
   if (EPI::kReduce) {
-    const bool lanes = UsesFastHop<SF>::value && std::is_same<IDX, IdxCompact>::value && t.lanes > 0;
-    launch_finalize(a.red, a.nrhs, grid_for(a.g, t, a.nrhs, npar), a.mask, st, lanes ? kLaneWarps : 1);
+    const bool lanes = (UsesFastHop<SF>::value || std::is_same<SF, SpinorField<P_DOUBLE>>::value) &&
+                       std::is_same<IDX, IdxCompact>::value && t.lanes > 0;
+    (void)lanes;  // lane kernels also write one partial per block
+    launch_finalize(a.red, a.nrhs, grid_for(a.g, t, a.nrhs, npar), a.mask, st, 1);
   }
 }
 
@@ -213,6 +215,17 @@ template <bool DAG, class IDX, class LF, class SF, class EPI>
 static void launch_hop_impl(const Tune& t, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st) {
   dim3 grid = grid_for(a.g, t, a.nrhs, npar), block(t.bx, t.by, 1);
   g_launches++;
+  if constexpr (std::is_same<SF, SpinorField<P_DOUBLE>>::value && std::is_same<IDX, IdxCompact>::value) {
+    if (t.lanes > 0) {  // FP64 fields stored RHS-innermost
+      dim3 lb(kLaneBlock, 1, 1);
+      switch (t.lanes) {
+        case 16: hop_lanes_d_kernel<DAG, 16><<<grid, lb, 0, st>>>(a); break;
+        case 8: hop_lanes_d_kernel<DAG, 8><<<grid, lb, 0, st>>>(a); break;
+        default: hop_lanes_d_kernel<DAG, 4><<<grid, lb, 0, st>>>(a); break;
+      }
+      return;
+    }
+  }
   if constexpr (UsesFastHop<SF>::value && std::is_same<IDX, IdxCompact>::value) {
     if (t.lanes > 0) {
       dim3 lb(kLaneBlock, 1, 1);
@@ -279,7 +292,7 @@ static void launch_site_lanes(int R, const Geom& g, int parity0, int npar, int n
     case 8: site_lanes_kernel<8><<<grid, block, 0, st>>>(a); break;
     default: site_lanes_kernel<4><<<grid, block, 0, st>>>(a); break;
   }
-  if (F::kReduce) launch_finalize(red, nrhs, grid, mask, st, kLaneWarps);
+  if (F::kReduce) launch_finalize(red, nrhs, grid, mask, st, 1);
 }
 
 // ============================================================== context
@@ -882,7 +895,7 @@ static void enqueue_iteration(wl_engine* E, cudaStream_t st, int part) {
       FAccumX<SFS> f;
       sf2<P_DOUBLE>(E->x64, f.x);
       sf2<S>(E->xs, f.xs);
-      launch_site(E->tsite, g, 0, E->npar, n, E->ru, f, Reduce{}, st);
+      launch_site_sloppy(E, 0, E->npar, n, E->ru, f, Reduce{}, st);
     }
     enqueue_true_residual<S>(E, E->ru, st);
     return;
@@ -945,7 +958,8 @@ static void enqueue_iteration(wl_engine* E, cudaStream_t st, int part) {
     }
   }
   g_launches++;
-  cg_decide_kernel<<<1, 128, 0, st>>>(Sc, n, E->use_cond ? 1 : 0, E->cond, E->use_cond ? E->ru_iters : nullptr);
+  cg_decide_kernel<<<1, 128, 0, st>>>(Sc, n, E->use_cond ? 1 : 0, E->cond, E->use_cond ? E->ru_iters : nullptr,
+                                      E->lanes_mode ? 1 : 0);
 }
 
 template <int S>
@@ -1086,6 +1100,7 @@ static void debug_apply_impl(wl_engine* E, int stage, double mass, const void* i
     FUnpack f;
     f.g = g;
     sf2<P_DOUBLE>(dst, f.in);
+    f.in_off = 0;
     f.out = sref(out, g);
     f.rhs_off = 0;
     launch_site(E->tsite, g, res_np == 1 ? res_par : 0, res_np, 1, nullptr, f, Reduce{}, st);
@@ -1303,11 +1318,13 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   cudaStream_t keep = ctx->stream;
   ctx->stream = st;
   const int tpar = prm->op == WL_SOLVE_EO_NORMAL ? 1 : 2;
-  if (s == WL_OK) s = alloc_field(ctx, E->b64, P_DOUBLE, g.Vh, n, E->npar);
-  if (s == WL_OK) s = alloc_field(ctx, E->x64, P_DOUBLE, g.Vh, n, E->npar);
-  if (s == WL_OK) s = alloc_field(ctx, E->y64, P_DOUBLE, g.Vh, n, E->npar);
-  if (s == WL_OK) s = alloc_field(ctx, E->t64, P_DOUBLE, g.Vh, n, tpar);
+  // in lanes mode the FP64 fields are RHS-innermost too: the reliable update
+  // then runs as one RHS-in-lanes FP64 pass over all slots
   const bool li = E->lanes_mode;
+  if (s == WL_OK) s = alloc_field(ctx, E->b64, P_DOUBLE, g.Vh, n, E->npar, li);
+  if (s == WL_OK) s = alloc_field(ctx, E->x64, P_DOUBLE, g.Vh, n, E->npar, li);
+  if (s == WL_OK) s = alloc_field(ctx, E->y64, P_DOUBLE, g.Vh, n, E->npar, li);
+  if (s == WL_OK) s = alloc_field(ctx, E->t64, P_DOUBLE, g.Vh, n, tpar, li);
   if (s == WL_OK) s = alloc_field(ctx, E->xs, E->sprec, g.Vh, n, E->npar, li);
   if (s == WL_OK) s = alloc_field(ctx, E->rs, E->sprec, g.Vh, n, E->npar, li);
   if (s == WL_OK) s = alloc_field(ctx, E->p, E->sprec, g.Vh, n, E->npar, li);
@@ -1352,6 +1369,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   E->h_maxiter.assign(n, E->prm.maxiter);
   E->ts = pick_tune(E, st);
   E->td = Tune{1, 128, 1};
+  if (E->lanes_mode) E->td.lanes = n > 8 ? 16 : (n > 4 ? 8 : 4);
   E->tsite = Tune{1, 128, 1};
   e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
@@ -1588,12 +1606,10 @@ static wl_status engine_unpack(wl_engine* E, int first, int count, void* x) {
   wl_ctx* ctx = E->ctx;
   cudaStream_t st = engine_stream(E);
   const Geom& g = ctx->g;
-  IField view = E->x64;
-  view.data = (char*)E->x64.data + (size_t)first * view.rstride() * 16;
-  view.nrhs = count;
   FUnpack f;
   f.g = g;
-  sf2<P_DOUBLE>(view, f.in);
+  sf2<P_DOUBLE>(E->x64, f.in);
+  f.in_off = first;
   f.out = sref(x, g);
   f.rhs_off = 0;
   launch_site(E->tsite, g, 0, E->npar, count, nullptr, f, Reduce{}, st);

@@ -207,8 +207,9 @@ WL_D void reduce_rhs(const double (&val)[NR], const Reduce& R, int nrhs, const i
 }
 
 // result[rhs] = sum_b partials[rhs][b] in a fixed order, for RHS in `mask`:
-// one 512-thread block per RHS, four independent accumulators per thread.
-constexpr int kFinalizeThreads = 512;
+// one 1024-thread block per RHS, eight independent accumulators per thread so
+// that enough loads are in flight to stream the partials at a useful rate.
+constexpr int kFinalizeThreads = 1024;
 
 __global__ void __launch_bounds__(kFinalizeThreads) reduce_finalize_kernel(Reduce R, int nrhs, int nblk,
                                                                             const int* mask) {
@@ -217,17 +218,15 @@ __global__ void __launch_bounds__(kFinalizeThreads) reduce_finalize_kernel(Reduc
   if (rhs >= nrhs) return;
   if (mask != nullptr && mask[rhs] == 0) return;  // uniform per block
   const double* p = R.partials + (long long)rhs * nblk;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  const int step = 4 * kFinalizeThreads;
+  double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  constexpr int step = 8 * kFinalizeThreads;
   int b = threadIdx.x;
-  for (; b + 3 * kFinalizeThreads < nblk; b += step) {
-    a0 += p[b];
-    a1 += p[b + kFinalizeThreads];
-    a2 += p[b + 2 * kFinalizeThreads];
-    a3 += p[b + 3 * kFinalizeThreads];
+  for (; b + 7 * kFinalizeThreads < nblk; b += step) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] += p[b + k * kFinalizeThreads];
   }
-  for (; b < nblk; b += kFinalizeThreads) a0 += p[b];
-  double v[1] = {(a0 + a1) + (a2 + a3)};
+  for (; b < nblk; b += kFinalizeThreads) a[0] += p[b];
+  double v[1] = {((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]))};
   block_sum<1>(v, sm);
   if (threadIdx.x == 0) R.result[rhs] = v[0];
 }

@@ -302,20 +302,28 @@ WL_D void lane_dir(const SF& src, const LinkSmem* Ls, const int* nbs, int rhs, f
   }
 }
 
-// Per-warp partial sums (no block barrier): after the xor-shuffles over the
-// sites of a warp, lanes 0..R-1 hold the warp's sum for RHS rbase + lane; warp
-// w of block b writes partials[rhs][b * 4 + w].
+// Per-block partial sums: xor-shuffles over the sites of a warp leave lanes
+// 0..R-1 with the warp's sum for RHS rbase + lane; after one barrier threads
+// 0..R-1 add the block's warps in a fixed order and block b writes
+// partials[rhs][b].  Every thread of the block must call this.
 constexpr int kLaneWarps = kLaneBlock / 32;
+static_assert(kLaneWarps == 4, "reduce_lanes adds four warps");
 
 template <int R>
 WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* /*mask*/) {
+  __shared__ double sred[kLaneWarps][32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 #pragma unroll
   for (int off = R; off < 32; off <<= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-  const int nblk = gridDim.x * gridDim.z * kLaneWarps;
-  const int blk = (blockIdx.z * gridDim.x + blockIdx.x) * kLaneWarps + warp;
-  const int rhs = blockIdx.y * R + lane;
-  if (lane < R && rhs < nrhs) Rd.partials[(long long)rhs * nblk + blk] = v;
+  if (lane < R) sred[warp][lane] = v;
+  __syncthreads();
+  if (tid < R) {
+    const double x = (sred[0][tid] + sred[1][tid]) + (sred[2][tid] + sred[3][tid]);
+    const int nblk = gridDim.x * gridDim.z;
+    const int blk = blockIdx.z * gridDim.x + blockIdx.x;
+    const int rhs = blockIdx.y * R + tid;
+    if (rhs < nrhs) Rd.partials[(long long)rhs * nblk + blk] = x;
+  }
 }
 
 template <bool DAG, int R, class LF, class SF, class EPI>
@@ -376,6 +384,148 @@ __global__ void __launch_bounds__(kLaneBlock) hop_lanes_kernel(HopArgs<LF, SF, E
 #pragma unroll
     for (int k = 0; k < 12; ++k) o.v[k / 3][k % 3] = {acc[k].x, acc[k].y};
     red = A.epi(rhs, parity, (long long)c, o);
+  }
+  if (EPI::kReduce) reduce_lanes<R>(red, A.red, A.nrhs, A.mask);
+}
+
+// ============================================================================
+// FP64 stencil with RHS in the lanes, for the reliable updates of the batched
+// solver (FP64 fields RHS-innermost).  Same two phases as hop_lanes_kernel:
+// each site's 8 links are reconstructed once per block into shared memory
+// (boundary phase folded in), then every lane applies them to its RHS.  The
+// spin projection is fused with the load, one colour at a time, so a full
+// FP64 source spinor is never live in registers; for mu = 3 only the two spin
+// rows the projector keeps are loaded.
+struct SiteLinksD {
+  double2 m[8][9];  // q = 2*mu + dir; element (a, b) at a*3 + b
+  double2 pad;      // 1168-byte stride: the sites of one warp hit different banks
+};
+
+template <int R>
+struct LaneSmemD {
+  static constexpr int S = kLaneBlock / R;
+  SiteLinksD link[S];
+  int nb[S][8];
+  int ok[S];
+};
+
+// h = (1 + C g_mu) psi(nb) rows 0,1 (mu = 3 without its factor 2, applied by the caller)
+template <int MU, int C>
+WL_D void load_project_d(const SpinorField<P_DOUBLE>& f, int rhs, unsigned nb, Half<double>& h) {
+#pragma unroll
+  for (int col = 0; col < 3; ++col) {
+    auto ld = [&](int sp) {
+      const double2 v = ldg(f.ptr + f.at(rhs, sp * 3 + col, nb));
+      return cplx<double>{v.x, v.y};
+    };
+    if (MU == 3) {
+      h.v[0][col] = C > 0 ? ld(0) : ld(2);
+      h.v[1][col] = C > 0 ? ld(1) : ld(3);
+      continue;
+    }
+    const cplx<double> s0 = ld(0), s1 = ld(1), s2 = ld(2), s3 = ld(3);
+    if (MU == 0) {
+      h.v[0][col] = C > 0 ? s0 + s3 : s0 - s3;
+      h.v[1][col] = C > 0 ? s1 + s2 : s1 - s2;
+    } else if (MU == 1) {
+      h.v[0][col] = C > 0 ? s0 + mul_mi(s3) : s0 + mul_i(s3);
+      h.v[1][col] = C > 0 ? s1 + mul_i(s2) : s1 + mul_mi(s2);
+    } else {
+      h.v[0][col] = C > 0 ? s0 + mul_mi(s2) : s0 + mul_i(s2);
+      h.v[1][col] = C > 0 ? s1 + mul_mi(s3) : s1 + mul_i(s3);
+    }
+  }
+}
+
+template <bool DAGU>
+WL_D void color_mul_smem_d(const double2 (&m)[9], const Half<double>& h, Half<double>& o) {
+#pragma unroll
+  for (int s = 0; s < 2; ++s)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      cplx<double> acc = {0.0, 0.0};
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const double2 u = DAGU ? m[b * 3 + a] : m[a * 3 + b];
+        if (DAGU) fmac_(acc, cplx<double>{u.x, u.y}, h.v[s][b]);
+        else fma_(acc, cplx<double>{u.x, u.y}, h.v[s][b]);
+      }
+      o.v[s][a] = acc;
+    }
+}
+
+template <int MU, bool DAG>
+WL_D void lane_dir_d(const SpinorField<P_DOUBLE>& src, const SiteLinksD& Ls, const int* nbs, int rhs,
+                     Spinor<double>& acc) {
+  constexpr int CF = DAG ? +1 : -1;
+  constexpr int CB = -CF;
+#pragma unroll
+  for (int dir = 0; dir < 2; ++dir) {
+    const int q = 2 * MU + dir;
+    Half<double> h, uh;
+    if (dir == 0) {
+      load_project_d<MU, CF>(src, rhs, (unsigned)nbs[q], h);
+      color_mul_smem_d<false>(Ls.m[q], h, uh);
+    } else {
+      load_project_d<MU, CB>(src, rhs, (unsigned)nbs[q], h);
+      color_mul_smem_d<true>(Ls.m[q], h, uh);
+    }
+    if (MU == 3) {
+#pragma unroll
+      for (int s = 0; s < 2; ++s)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) uh.v[s][a] = 2.0 * uh.v[s][a];
+    }
+    if (dir == 0) spin_accum<MU, CF>(acc, uh);
+    else spin_accum<MU, CB>(acc, uh);
+  }
+}
+
+template <bool DAG, int R, class LF, class EPI>
+__global__ void __launch_bounds__(kLaneBlock, 4) hop_lanes_d_kernel(HopArgs<LF, SpinorField<P_DOUBLE>, EPI> A) {
+  constexpr int S = kLaneBlock / R;
+  __shared__ LaneSmemD<R> sm;
+  const int tid = threadIdx.x;
+  const int parity = A.parity0 ^ blockIdx.z;
+  const int site0 = blockIdx.x * S;
+  for (int j = tid; j < 8 * S; j += kLaneBlock) {
+    const int sl = j >> 3, q = j & 7, mu = q >> 1, dir = q & 1;
+    const int c = site0 + sl;
+    if (c < A.g.Vh) {
+      const Site s = site_from_compact(A.g, parity, c);
+      const int nb = neighbor(A.g, s, mu, dir == 0 ? +1 : -1);
+      Link<double> u;
+      if (dir == 0) A.links.load(u, parity, mu, c);
+      else A.links.load(u, 1 - parity, mu, nb);
+      const bool ph = A.g.ph_on[mu] && (dir == 0 ? (s.x[mu] == A.g.L[mu] - 1) : (s.x[mu] == 0));
+      if (ph) {
+        const cplx<double> w{A.g.ph_re[mu], A.g.ph_im[mu]};
+#pragma unroll
+        for (int k = 0; k < 9; ++k) u.m[k / 3][k % 3] = u.m[k / 3][k % 3] * w;
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) sm.link[sl].m[q][k] = make_double2(u.m[k / 3][k % 3].re, u.m[k / 3][k % 3].im);
+      sm.nb[sl][q] = nb;
+      if (q == 0) sm.ok[sl] = 1;
+    } else if (q == 0) {
+      sm.ok[sl] = 0;
+    }
+  }
+  __syncthreads();
+  const int sl = tid / R;
+  const int c = site0 + sl;
+  const int rhs = blockIdx.y * R + (tid % R);
+  double red = 0.0;
+  const bool act = sm.ok[sl] && rhs < A.nrhs && (A.mask == nullptr || A.mask[rhs] != 0);
+  if (act) {
+    Spinor<double> acc;
+    zero(acc);
+    const SpinorField<P_DOUBLE>& src = A.src[1 - parity];
+    lane_dir_d<0, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
+    lane_dir_d<1, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
+    lane_dir_d<2, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
+    lane_dir_d<3, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
+    red = A.epi(rhs, parity, (long long)c, acc);
   }
   if (EPI::kReduce) reduce_lanes<R>(red, A.red, A.nrhs, A.mask);
 }

@@ -76,10 +76,11 @@ struct FUnpack {
   SpinorField<P_DOUBLE> in[2];
   SpinorRef out;  // out-field index = rhs - rhs_off
   int rhs_off;
+  int in_off;     // in-field index = rhs + in_off
   WL_D double operator()(int rhs, int parity, int c) const {
     const long long f = flat_of(g, parity, c);
     Spinor<double> s;
-    in[parity].load(s, rhs, c);
+    in[parity].load(s, rhs + in_off, c);
     out.store(s, rhs - rhs_off, f);
     return 0.0;
   }
@@ -333,7 +334,12 @@ enum SlotStatus { ST_IDLE = 0, ST_RUNNING = 1, ST_CONVERGED = 2, ST_MAXITER = 3,
 // with a conditional node (`use_cond`), also switches the node's body (the FP64
 // true-residual kernels) on only when at least one slot needs it, and counts
 // such iterations in *ru_iters.
-__global__ void cg_decide_kernel(CGScalars S, int n, int use_cond, cudaGraphConditionalHandle cond, int* ru_iters) {
+// Reliable-update decision per slot.  With `group` set, one slot's trigger
+// sends every active slot through the update: the batched FP64 update costs
+// the same for one slot as for all, and updating together keeps the slots'
+// update schedules aligned instead of staggered over many iterations.
+__global__ void cg_decide_kernel(CGScalars S, int n, int use_cond, cudaGraphConditionalHandle cond, int* ru_iters,
+                                 int group) {
   __shared__ int any;
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
@@ -357,6 +363,9 @@ __global__ void cg_decide_kernel(CGScalars S, int n, int use_cond, cudaGraphCond
     if (trig) atomicOr(&any, 1);
   }
   __syncthreads();
+  if (group && any)
+    for (int s = threadIdx.x; s < n; s += blockDim.x)
+      if (S.active[s]) S.ru[s] = 1;
   if (threadIdx.x == 0) {
     if (any && ru_iters) *ru_iters += 1;
     if (use_cond) cudaGraphSetConditional(cond, any ? 1u : 0u);
