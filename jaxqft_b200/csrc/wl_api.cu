@@ -629,7 +629,7 @@ struct wl_engine {
   // scalars (device)
   double* dbl = nullptr;
   int* ints = nullptr;
-  double *r2, *r2_new, *pAp, *r2_true, *rmax2, *b2, *tol2, *beta, *one, *neg_half, *half_alpha, *m0;
+  double *r2, *r2_new, *pAp, *r2_true, *rmax2, *b2, *tol2, *beta, *one, *neg_half, *half_alpha, *m0, *alpha;
   int *active, *ru, *iters, *maxiter, *status, *n_ru, *n_active, *admit;
   // host mirrors of parameters
   std::vector<double> h_tol2, h_one, h_neg_half, h_half_alpha, h_m0;
@@ -661,7 +661,7 @@ static cudaStream_t engine_stream(const wl_engine* E) {
   return g_engine_streams[E];
 }
 
-static const int kEngineDoubles = 12;
+static const int kEngineDoubles = 13;
 static const int kEngineInts = 8;
 
 int64_t engine_bytes_impl(const Geom& g, int op, int sprec, int n) {
@@ -689,7 +689,7 @@ extern "C" int64_t wl_engine_bytes(const wl_ctx* ctx, int op, int inner_prec, in
 }
 
 static Reduce red_to(wl_engine* E, double* result) {
-  Reduce r;
+  Reduce r{};
   r.partials = E->partials;
   r.counter = E->counters;
   r.result = result;
@@ -923,6 +923,8 @@ static void enqueue_iteration(wl_engine* E, cudaStream_t st, int part) {
       sf2<S>(E->y, A.epi.out); sf2<S>(E->p, A.epi.self); A.epi.has_self = 1;
       A.epi.a = E->one; A.epi.b = E->half_alpha;
       A.red = red_to(E, E->pAp);
+      A.red.num = E->r2;
+      A.red.quot = E->alpha;  // alpha = r2 / pAp for the fused CG update
       launch_hop<false, IdxCompact>(E->ts, A, 1, st);
     }
     {  // t2 = Kdag_oe y
@@ -935,7 +937,7 @@ static void enqueue_iteration(wl_engine* E, cudaStream_t st, int part) {
       HopArgs<LS, SFS, EpiCG<SFS>> A{};
       A.g = g; A.links = L; sf2<S>(E->t1, A.src); A.parity0 = 0; A.nrhs = n; A.mask = E->active;
       sf2<S>(E->y, A.epi.y); sf2<S>(E->p, A.epi.p); sf2<S>(E->xs, A.epi.xs); sf2<S>(E->rs, A.epi.rs);
-      A.epi.a = E->one; A.epi.b = E->half_alpha; A.epi.r2 = E->r2; A.epi.pAp = E->pAp;
+      A.epi.a = E->one; A.epi.b = E->half_alpha; A.epi.r2 = E->r2; A.epi.pAp = E->pAp; A.epi.alpha = E->alpha;
       A.red = red_to(E, E->r2_new);
       launch_hop<true, IdxCompact>(E->ts, A, 1, st);
     }
@@ -946,13 +948,15 @@ static void enqueue_iteration(wl_engine* E, cudaStream_t st, int part) {
       sf2<S>(E->y, A.epi.out); sf2<S>(E->p, A.epi.self); A.epi.has_self = 1;
       A.epi.a = E->m0; A.epi.b = E->neg_half;
       A.red = red_to(E, E->pAp);
+      A.red.num = E->r2;
+      A.red.quot = E->alpha;  // alpha = r2 / pAp for the fused CG update
       launch_hop<false, IdxCompact>(E->ts, A, 2, st);
     }
     {  // Ap = D^dag y ; CG update
       HopArgs<LS, SFS, EpiCG<SFS>> A{};
       A.g = g; A.links = L; sf2<S>(E->y, A.src); A.parity0 = 0; A.nrhs = n; A.mask = E->active;
       sf2<S>(E->y, A.epi.y); sf2<S>(E->p, A.epi.p); sf2<S>(E->xs, A.epi.xs); sf2<S>(E->rs, A.epi.rs);
-      A.epi.a = E->m0; A.epi.b = E->neg_half; A.epi.r2 = E->r2; A.epi.pAp = E->pAp;
+      A.epi.a = E->m0; A.epi.b = E->neg_half; A.epi.r2 = E->r2; A.epi.pAp = E->pAp; A.epi.alpha = E->alpha;
       A.red = red_to(E, E->r2_new);
       launch_hop<true, IdxCompact>(E->ts, A, 2, st);
     }
@@ -1357,6 +1361,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   E->r2 = d + 0 * n; E->r2_new = d + 1 * n; E->pAp = d + 2 * n; E->r2_true = d + 3 * n;
   E->rmax2 = d + 4 * n; E->b2 = d + 5 * n; E->tol2 = d + 6 * n; E->beta = d + 7 * n;
   E->one = d + 8 * n; E->neg_half = d + 9 * n; E->half_alpha = d + 10 * n; E->m0 = d + 11 * n;
+  E->alpha = d + 12 * n;
   int* I = E->ints;
   E->active = I + 0 * n; E->ru = I + 1 * n; E->iters = I + 2 * n; E->maxiter = I + 3 * n;
   E->status = I + 4 * n; E->n_ru = I + 5 * n; E->admit = I + 6 * n; E->n_active = I + 8 * n;

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <stdint.h>
+#include <type_traits>
 
 #define WL_HD __host__ __device__ __forceinline__
 #define WL_D __device__ __forceinline__
@@ -265,6 +266,78 @@ template <> struct SpinorField<P_HALF> : Strides {
     }
   }
 };
+
+// ---------------------------------------------------------------- packed FP32x2 I/O
+// A spinor as 12 float2 (re, im), component k = spin*3 + colour, for the
+// sm_100 packed FP32x2 pipe (__ffma2_rn / __fmul2_rn: two lanes per instruction).
+WL_D float2 f2(float a, float b) { return make_float2(a, b); }
+WL_D float2 swp(float2 v) { return make_float2(v.y, v.x); }
+WL_D float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+WL_D float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
+// load: v = stored values, returns the scale (value = scale * v; FP16 per-site norm)
+// store: v = values; FP16 stores pick the per-site norm max|v| and pack pairs
+template <class SF> struct Packed;
+
+template <> struct Packed<SpinorField<P_SINGLE>> {
+  WL_D static float load(const SpinorField<P_SINGLE>& f, int rhs, unsigned c, float2 (&v)[12]) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float4 q = ldg(f.ptr + f.at(rhs, k, c));
+      v[2 * k] = f2(q.x, q.y);
+      v[2 * k + 1] = f2(q.z, q.w);
+    }
+    return 1.0f;
+  }
+  WL_D static void store(const SpinorField<P_SINGLE>& f, int rhs, unsigned c, const float2 (&v)[12]) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) f.ptr[f.at(rhs, k, c)] = make_float4(v[2 * k].x, v[2 * k].y, v[2 * k + 1].x, v[2 * k + 1].y);
+  }
+};
+
+template <> struct Packed<SpinorField<P_HALF>> {
+  WL_D static float load(const SpinorField<P_HALF>& f, int rhs, unsigned c, float2 (&v)[12]) {
+    const float n = ldg(f.norm + f.nat(rhs, c));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const uint4 q = ldg(f.ptr + f.at(rhs, k, c));
+      v[4 * k + 0] = h2f(q.x);
+      v[4 * k + 1] = h2f(q.y);
+      v[4 * k + 2] = h2f(q.z);
+      v[4 * k + 3] = h2f(q.w);
+    }
+    return n;
+  }
+  WL_D static void store(const SpinorField<P_HALF>& f, int rhs, unsigned c, const float2 (&v)[12]) {
+    float mx = 0.f;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) mx = fmaxf(mx, fmaxf(fabsf(v[k].x), fabsf(v[k].y)));
+    // below FLT_MIN the site is stored as zero (1/mx would overflow, 0 * Inf = NaN)
+    const bool keep = mx >= 1.17549435e-38f;
+    const float inv = keep ? 1.0f / mx : 0.f;
+    f.norm[f.nat(rhs, c)] = keep ? mx : 0.f;
+    const float2 s = f2(inv, inv);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float2 a0 = fmul2(s, v[4 * k]), a1 = fmul2(s, v[4 * k + 1]);
+      const float2 a2 = fmul2(s, v[4 * k + 2]), a3 = fmul2(s, v[4 * k + 3]);
+      uint4 q;
+      q.x = f2h(a0.x, a0.y);
+      q.y = f2h(a1.x, a1.y);
+      q.z = f2h(a2.x, a2.y);
+      q.w = f2h(a3.x, a3.y);
+      f.ptr[f.at(rhs, k, c)] = q;
+    }
+  }
+};
+
+// |v|^2 of a packed spinor, accumulated in FP32 pairs
+WL_D double pnorm2(const float2 (&v)[12]) {
+  float2 s = f2(0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 12; ++k) s = ffma2(v[k], v[k], s);
+  return (double)s.x + (double)s.y;
+}
 
 // Spinor field in the reference layout: complex128 [rhs][V][4][3], site = flat index.
 struct SpinorRef {

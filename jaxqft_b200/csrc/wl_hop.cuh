@@ -176,6 +176,8 @@ struct Reduce {
   double* partials;   // [nrhs][nblk]
   unsigned* counter;  // unused (kept for layout stability)
   double* result;     // [nrhs]
+  const double* num;  // optional: quot[rhs] = num[rhs] / result[rhs] (0 when result <= 0)
+  double* quot;
 };
 
 constexpr int kMaxRB = 16;  // RHS per block (BY * NR)
@@ -228,7 +230,10 @@ __global__ void __launch_bounds__(kFinalizeThreads) reduce_finalize_kernel(Reduc
   for (; b < nblk; b += kFinalizeThreads) a[0] += p[b];
   double v[1] = {((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]))};
   block_sum<1>(v, sm);
-  if (threadIdx.x == 0) R.result[rhs] = v[0];
+  if (threadIdx.x == 0) {
+    R.result[rhs] = v[0];
+    if (R.quot) R.quot[rhs] = v[0] > 0.0 ? R.num[rhs] / v[0] : 0.0;
+  }
 }
 
 // Generic launch parameters
@@ -326,6 +331,23 @@ struct EpiXpay {
     }
     out[parity].store(o, rhs, idx);
     return RED ? snorm2(o) : 0.0;
+  }
+  // same on packed FP32 pairs (FP16/FP32 fields, RHS-in-lanes kernels)
+  WL_D double packed(int rhs, int parity, unsigned idx, float2 (&acc)[12]) const {
+    const float bb = float(b ? b[rhs] : b0);
+    const float2 b2 = f2(bb, bb);
+    if (has_self) {
+      float2 x[12];
+      const float sx = Packed<SF>::load(self[parity], rhs, idx, x) * float(a ? a[rhs] : a0);
+      const float2 s2 = f2(sx, sx);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) acc[k] = ffma2(b2, acc[k], fmul2(s2, x[k]));
+    } else {
+#pragma unroll
+      for (int k = 0; k < 12; ++k) acc[k] = fmul2(b2, acc[k]);
+    }
+    Packed<SF>::store(out[parity], rhs, idx, acc);
+    return RED ? pnorm2(acc) : 0.0;
   }
 };
 

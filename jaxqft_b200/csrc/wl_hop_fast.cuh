@@ -11,11 +11,6 @@
 
 namespace wl {
 
-WL_D float2 f2(float a, float b) { return make_float2(a, b); }
-WL_D float2 swp(float2 v) { return make_float2(v.y, v.x); }
-WL_D float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-WL_D float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-
 // Raw spinor load: values without the FP16 per-site norm (returned separately).
 template <class SF> struct RawLoad;
 
@@ -380,10 +375,7 @@ __global__ void __launch_bounds__(kLaneBlock) hop_lanes_kernel(HopArgs<LF, SF, E
     lane_dir<1, DAG>(src, Ls, nbs, rhs, acc);
     lane_dir<2, DAG>(src, Ls, nbs, rhs, acc);
     lane_dir<3, DAG>(src, Ls, nbs, rhs, acc);
-    Spinor<float> o;
-#pragma unroll
-    for (int k = 0; k < 12; ++k) o.v[k / 3][k % 3] = {acc[k].x, acc[k].y};
-    red = A.epi(rhs, parity, (long long)c, o);
+    red = A.epi.packed(rhs, parity, (unsigned)c, acc);
   }
   if (EPI::kReduce) reduce_lanes<R>(red, A.red, A.nrhs, A.mask);
 }

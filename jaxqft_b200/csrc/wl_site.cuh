@@ -169,11 +169,21 @@ struct FUpdateP {
   const double* beta;
   WL_D double operator()(int rhs, int parity, int c) const {
     using T = typename SFS::real;
-    Spinor<T> r, pv, o;
-    rs[parity].load_plain(r, rhs, c);
-    p[parity].load_plain(pv, rhs, c);
-    axpby(o, T(1), r, T(beta[rhs]), pv);
-    p[parity].store(o, rhs, c);
+    if constexpr (std::is_same<T, float>::value) {  // packed FP32 pairs
+      float2 r[12], pv[12];
+      const float sr = Packed<SFS>::load(rs[parity], rhs, (unsigned)c, r);
+      const float sp = Packed<SFS>::load(p[parity], rhs, (unsigned)c, pv) * float(beta[rhs]);
+      const float2 r2 = f2(sr, sr), p2 = f2(sp, sp);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) pv[k] = ffma2(p2, pv[k], fmul2(r2, r[k]));
+      Packed<SFS>::store(p[parity], rhs, (unsigned)c, pv);
+    } else {
+      Spinor<T> r, pv, o;
+      rs[parity].load_plain(r, rhs, c);
+      p[parity].load_plain(pv, rhs, c);
+      axpby(o, T(1), r, T(beta[rhs]), pv);
+      p[parity].store(o, rhs, c);
+    }
     return 0.0;
   }
 };
@@ -189,6 +199,7 @@ struct EpiCG {
   const double* b;
   const double* r2;
   const double* pAp;
+  const double* alpha;  // r2 / pAp per RHS (written by the pAp reduction), packed path
   WL_D double operator()(int rhs, int parity, long long idx, Spinor<typename SF::real>& acc) const {
     using T = typename SF::real;
     const double den = pAp[rhs];
@@ -210,6 +221,37 @@ struct EpiCG {
     xs[parity].store(xv, rhs, idx);
     rs[parity].store(rv, rhs, idx);
     return snorm2(rv);
+  }
+  // same on packed FP32 pairs; the order keeps at most two packed spinors live
+  WL_D double packed(int rhs, int parity, unsigned idx, float2 (&acc)[12]) const {
+    const float al = float(alpha[rhs]);
+    const float bb = float(b[rhs]);
+    const float2 b2 = f2(bb, bb), nal = f2(-al, -al);
+    float2 v[12];
+    {  // acc <- Ap = a*y + b*acc
+      const float sy = Packed<SF>::load(y[parity], rhs, idx, v) * float(a[rhs]);
+      const float2 s2 = f2(sy, sy);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) acc[k] = ffma2(b2, acc[k], fmul2(s2, v[k]));
+    }
+    double n;
+    {  // rs <- rs - alpha Ap
+      const float sr = Packed<SF>::load(rs[parity], rhs, idx, v);
+      const float2 s2 = f2(sr, sr);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) v[k] = ffma2(nal, acc[k], fmul2(s2, v[k]));
+      Packed<SF>::store(rs[parity], rhs, idx, v);
+      n = pnorm2(v);
+    }
+    {  // xs <- xs + alpha p
+      const float sp = Packed<SF>::load(p[parity], rhs, idx, acc) * al;
+      const float sx = Packed<SF>::load(xs[parity], rhs, idx, v);
+      const float2 p2 = f2(sp, sp), x2 = f2(sx, sx);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) v[k] = ffma2(p2, acc[k], fmul2(x2, v[k]));
+      Packed<SF>::store(xs[parity], rhs, idx, v);
+    }
+    return n;
   }
 };
 
