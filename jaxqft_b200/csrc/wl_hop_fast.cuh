@@ -225,14 +225,21 @@ __global__ void __launch_bounds__(256) hop_fast_kernel(HopArgs<LF, SF, EPI> A) {
 
 // ============================================================================
 // Multi-RHS hop with RHS in the lanes.  A block of 128 threads covers
-// S = 128 / R sites x R right-hand sides (lane = rhs + R * site).  Phase 1: the
-// block reconstructs the 8 links of each of its sites once into shared memory
-// as packed pairs (boundary phase folded in) together with the neighbour
-// indices.  Phase 2: every lane runs the stencil for its (site, RHS), reading
+// S = 128 / R sites x R right-hand sides (lane = rhs + R * site).  Phase 1:
+// each warp reconstructs the 8 links of each of its 32/R sites once into shared
+// memory as packed pairs (boundary phase folded in) together with the
+// neighbour indices; a warp barrier (not a block barrier) ends the phase.
+// Phase 2: every lane runs the stencil for its (site, RHS), reading
 // the site's links as shared-memory broadcasts.  Spinor loads stay
 // sector-efficient: lanes r of sites c and c+1 read the two 16-byte halves of
 // one 32-byte sector.
 constexpr int kLaneBlock = 128;
+// Resident blocks per SM the FP32-arithmetic lane kernel is compiled for:
+// 8 caps it at 64 registers (32 warps per SM) to hide the L2 latency of the
+// neighbour gathers.
+#ifndef WL_LANE_MIN_BLOCKS
+#define WL_LANE_MIN_BLOCKS 8
+#endif
 
 struct LinkSmem {
   float4 p[9];  // (R.x, R.y, I.x, I.y) for element (a, b) = k / 3, k % 3
@@ -322,15 +329,19 @@ WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* /*mask*/
 }
 
 template <bool DAG, int R, class LF, class SF, class EPI>
-__global__ void __launch_bounds__(kLaneBlock) hop_lanes_kernel(HopArgs<LF, SF, EPI> A) {
+__global__ void __launch_bounds__(kLaneBlock, WL_LANE_MIN_BLOCKS) hop_lanes_kernel(HopArgs<LF, SF, EPI> A) {
   constexpr int S = kLaneBlock / R;
   __shared__ LaneSmem<R> sm;
   const int tid = threadIdx.x;
   const int parity = A.parity0 ^ blockIdx.z;
   const int site0 = blockIdx.x * S;
-  // ---- phase 1: links (phase-folded packed pairs) and neighbour indices
-  for (int j = tid; j < 8 * S; j += kLaneBlock) {
-    const int sl = j >> 3, q = j & 7, mu = q >> 1, dir = q & 1;
+  // ---- phase 1: links (phase-folded packed pairs) and neighbour indices.
+  // Each warp stages the links of its own 32/R sites, so only a warp barrier
+  // separates the phases and warps of one block do not wait for each other.
+  constexpr int SPW = 32 / R;
+  const int wsite = (tid >> 5) * SPW;
+  for (int j = tid & 31; j < 8 * SPW; j += 32) {
+    const int sl = wsite + (j >> 3), q = j & 7, mu = q >> 1, dir = q & 1;
     const int c = site0 + sl;
     if (c < A.g.Vh) {
       const Site s = site_from_compact(A.g, parity, c);
@@ -357,8 +368,8 @@ __global__ void __launch_bounds__(kLaneBlock) hop_lanes_kernel(HopArgs<LF, SF, E
       sm.ok[sl] = 0;
     }
   }
-  __syncthreads();
-  // ---- phase 2: stencil for (site, rhs) of this lane
+  __syncwarp();
+  // ---- phase 2: stencil for (site, rhs) of this lane (a site of this warp)
   const int sl = tid / R;
   const int c = site0 + sl;
   const int rhs = blockIdx.y * R + (tid % R);
@@ -480,8 +491,10 @@ __global__ void __launch_bounds__(kLaneBlock, 4) hop_lanes_d_kernel(HopArgs<LF, 
   const int tid = threadIdx.x;
   const int parity = A.parity0 ^ blockIdx.z;
   const int site0 = blockIdx.x * S;
-  for (int j = tid; j < 8 * S; j += kLaneBlock) {
-    const int sl = j >> 3, q = j & 7, mu = q >> 1, dir = q & 1;
+  constexpr int SPW = 32 / R;  // sites per warp: each warp stages its own links
+  const int wsite = (tid >> 5) * SPW;
+  for (int j = tid & 31; j < 8 * SPW; j += 32) {
+    const int sl = wsite + (j >> 3), q = j & 7, mu = q >> 1, dir = q & 1;
     const int c = site0 + sl;
     if (c < A.g.Vh) {
       const Site s = site_from_compact(A.g, parity, c);
@@ -503,7 +516,7 @@ __global__ void __launch_bounds__(kLaneBlock, 4) hop_lanes_d_kernel(HopArgs<LF, 
       sm.ok[sl] = 0;
     }
   }
-  __syncthreads();
+  __syncwarp();
   const int sl = tid / R;
   const int c = site0 + sl;
   const int rhs = blockIdx.y * R + (tid % R);
