@@ -199,6 +199,28 @@ wl_status wl_apply_schur_normal_noalloc(wl_ctx* ctx, wl_gauge* gauge, double mas
 wl_status wl_pf_force(wl_ctx* ctx, wl_gauge* gauge, const void* X, const void* Y, double coef,
                       int accumulate, void* F);
 
+/* Gauge sector (HMC pure-gauge pieces) ------------------------------------ */
+/* Links / momenta in the reference layout BMXYIJ: complex128
+   [batch][4][Lx][Ly][Lz][Lt][3][3], periodic boundaries (the fermion BC of the
+   context does not apply).  All FP64. */
+
+/* F = -(beta/3) TA(U_mu(x) V_mu(x)^dag), V the sum of the six staples
+   (jaxqft/models/su3_ym.py:298-327 _staple / force_reference; su3_ym.py:96-123
+   the BMXYIJ form).  F has U's shape. */
+wl_status wl_gauge_force(wl_ctx* ctx, const void* U, int batch, double beta, void* F);
+
+/* Uout = exp(dt P) U per link (su3_ym.py:349-350 evolve_q_reference with
+   exp_method "expm", su3_ym.py:265-272).  Uout may alias U. */
+wl_status wl_gauge_evolve(wl_ctx* ctx, const void* P, const void* U, int batch, double dt, void* Uout);
+
+/* plaq_sum[b] = sum_{x, mu<nu} Re Tr U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
+   (host array; su3_ym.py:274-286 action = -(beta/3) plaq_sum, 369-388
+   average_plaquette = plaq_sum / (3 V 6)).  Synchronises the context stream. */
+wl_status wl_gauge_plaquette_sum(wl_ctx* ctx, const void* U, int batch, double* plaq_sum);
+
+/* kin[b] = -1/2 sum Re Tr P P (host array; su3_ym.py:362-364).  Synchronises. */
+wl_status wl_momentum_kinetic(wl_ctx* ctx, const void* P, int batch, double* kin);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,6 +17,7 @@
 
 #include "../../include/wilson_sm100.h"
 #include "wl_force.cuh"
+#include "wl_gauge.cuh"
 #include "wl_hop_fast.cuh"
 #include "wl_site.cuh"
 
@@ -31,6 +32,9 @@ struct wl_ctx {
   // scratch for reference-layout operator chains (temp full fields)
   void* tmp = nullptr;
   size_t tmp_bytes = 0;
+  // scratch for the gauge-sector reductions (block partials + per-batch results)
+  double* red = nullptr;
+  size_t red_bytes = 0;
 };
 
 struct wl_gauge {
@@ -333,6 +337,7 @@ extern "C" void wl_ctx_destroy(wl_ctx* ctx) {
   cudaSetDevice(ctx->device);
   wl_release_solve_cache(ctx);
   if (ctx->tmp) cudaFree(ctx->tmp);
+  if (ctx->red) cudaFree(ctx->red);
   delete ctx;
 }
 
@@ -597,6 +602,95 @@ extern "C" wl_status wl_pf_force(wl_ctx* ctx, wl_gauge* G, const void* X, const 
   g_launches++;
   pf_force_kernel<<<grid, 128, 0, ctx->stream>>>(A);
   return check_launch(ctx, "pf_force_kernel");
+}
+
+// ============================================================== gauge sector
+static wl_status ensure_red(wl_ctx* ctx, size_t bytes) {
+  if (ctx->red_bytes >= bytes) return WL_OK;
+  if (ctx->red) {
+    cudaFree(ctx->red);
+    ctx->red = nullptr;
+    ctx->red_bytes = 0;
+  }
+  WL_CUDA(ctx, cudaMalloc(&ctx->red, bytes));
+  ctx->red_bytes = bytes;
+  return WL_OK;
+}
+
+// Sum of per-block partials [batch][nblk] -> host out[batch] (fixed order).
+static wl_status finish_sums(wl_ctx* ctx, int batch, int nblk, double scale, double* out) {
+  Reduce r{};
+  r.partials = ctx->red;
+  r.result = ctx->red + (size_t)batch * nblk;
+  g_launches++;
+  reduce_finalize_kernel<<<batch, kFinalizeThreads, 0, ctx->stream>>>(r, batch, nblk, nullptr);
+  wl_status s = check_launch(ctx, "reduce_finalize_kernel");
+  if (s != WL_OK) return s;
+  std::vector<double> h(batch);
+  WL_CUDA(ctx, cudaMemcpyAsync(h.data(), r.result, sizeof(double) * batch, cudaMemcpyDeviceToHost, ctx->stream));
+  WL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int b = 0; b < batch; ++b) out[b] = scale * h[b];
+  return WL_OK;
+}
+
+static GaugeArgs gauge_args(wl_ctx* ctx, const void* U, const void* P, void* out, int batch, double coef) {
+  GaugeArgs A{};
+  A.g = ctx->g;
+  A.U = (const double2*)U;
+  A.P = (const double2*)P;
+  A.out = (double2*)out;
+  A.batch = batch;
+  A.coef = coef;
+  A.partials = ctx->red;
+  return A;
+}
+
+extern "C" wl_status wl_gauge_force(wl_ctx* ctx, const void* U, int batch, double beta, void* F) {
+  if (!ctx || !U || !F || batch < 1) WL_FAIL(ctx, WL_ERR_ARG, "null argument or batch < 1");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  GaugeArgs A = gauge_args(ctx, U, nullptr, F, batch, -beta / 3.0);
+  dim3 grid((ctx->g.V + 127) / 128, 4, batch);
+  g_launches++;
+  gauge_force_kernel<<<grid, 128, 0, ctx->stream>>>(A);
+  return check_launch(ctx, "gauge_force_kernel");
+}
+
+extern "C" wl_status wl_gauge_evolve(wl_ctx* ctx, const void* P, const void* U, int batch, double dt, void* Uout) {
+  if (!ctx || !P || !U || !Uout || batch < 1) WL_FAIL(ctx, WL_ERR_ARG, "null argument or batch < 1");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  GaugeArgs A = gauge_args(ctx, U, P, Uout, batch, dt);
+  const long long nl = (long long)batch * 4 * ctx->g.V;
+  g_launches++;
+  gauge_evolve_kernel<<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(A);
+  return check_launch(ctx, "gauge_evolve_kernel");
+}
+
+extern "C" wl_status wl_gauge_plaquette_sum(wl_ctx* ctx, const void* U, int batch, double* plaq_sum) {
+  if (!ctx || !U || !plaq_sum || batch < 1) WL_FAIL(ctx, WL_ERR_ARG, "null argument or batch < 1");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int nblk = (ctx->g.V + 127) / 128;
+  wl_status s = ensure_red(ctx, sizeof(double) * ((size_t)batch * nblk + batch));
+  if (s != WL_OK) return s;
+  GaugeArgs A = gauge_args(ctx, U, nullptr, nullptr, batch, 0.0);
+  g_launches++;
+  gauge_plaquette_kernel<<<dim3(nblk, 1, batch), 128, 0, ctx->stream>>>(A);
+  s = check_launch(ctx, "gauge_plaquette_kernel");
+  if (s != WL_OK) return s;
+  return finish_sums(ctx, batch, nblk, 1.0, plaq_sum);
+}
+
+extern "C" wl_status wl_momentum_kinetic(wl_ctx* ctx, const void* P, int batch, double* kin) {
+  if (!ctx || !P || !kin || batch < 1) WL_FAIL(ctx, WL_ERR_ARG, "null argument or batch < 1");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int nblk = (int)((4LL * ctx->g.V + 127) / 128);
+  wl_status s = ensure_red(ctx, sizeof(double) * ((size_t)batch * nblk + batch));
+  if (s != WL_OK) return s;
+  GaugeArgs A = gauge_args(ctx, nullptr, P, nullptr, batch, 0.0);
+  g_launches++;
+  gauge_kinetic_kernel<<<dim3(nblk, 1, batch), 128, 0, ctx->stream>>>(A);
+  s = check_launch(ctx, "gauge_kinetic_kernel");
+  if (s != WL_OK) return s;
+  return finish_sums(ctx, batch, nblk, 1.0, kin);
 }
 
 // ============================================================== CG engine

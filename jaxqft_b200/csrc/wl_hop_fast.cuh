@@ -392,6 +392,10 @@ __global__ void __launch_bounds__(kLaneBlock, WL_LANE_MIN_BLOCKS) hop_lanes_kern
 }
 
 // ============================================================================
+#ifndef WL_LANE_D_MIN_BLOCKS
+#define WL_LANE_D_MIN_BLOCKS 4  // resident blocks per SM the FP64 lane kernel is compiled for (128 registers)
+#endif
+
 // FP64 stencil with RHS in the lanes, for the reliable updates of the batched
 // solver (FP64 fields RHS-innermost).  Same two phases as hop_lanes_kernel:
 // each site's 8 links are reconstructed once per block into shared memory
@@ -412,21 +416,28 @@ struct LaneSmemD {
   int ok[S];
 };
 
-// h = (1 + C g_mu) psi(nb) rows 0,1 (mu = 3 without its factor 2, applied by the caller)
+// h = (1 + C g_mu) psi(nb) rows 0,1 (mu = 3 without its factor 2, applied by the
+// caller).  All loads of the direction are issued before any is used (12, or 6
+// for mu = 3), so each thread keeps a whole source spinor's worth of requests in
+// flight: at 16 warps per SM this is what hides the L2/HBM latency.
 template <int MU, int C>
 WL_D void load_project_d(const SpinorField<P_DOUBLE>& f, int rhs, unsigned nb, Half<double>& h) {
+  constexpr int s_lo = (MU == 3 && C < 0) ? 2 : 0;
+  constexpr int s_hi = (MU == 3 && C > 0) ? 2 : 4;
+  double2 v[4][3];
+#pragma unroll
+  for (int sp = s_lo; sp < s_hi; ++sp)
+#pragma unroll
+    for (int col = 0; col < 3; ++col) v[sp][col] = ldg(f.ptr + f.at(rhs, sp * 3 + col, nb));
 #pragma unroll
   for (int col = 0; col < 3; ++col) {
-    auto ld = [&](int sp) {
-      const double2 v = ldg(f.ptr + f.at(rhs, sp * 3 + col, nb));
-      return cplx<double>{v.x, v.y};
-    };
     if (MU == 3) {
-      h.v[0][col] = C > 0 ? ld(0) : ld(2);
-      h.v[1][col] = C > 0 ? ld(1) : ld(3);
+      h.v[0][col] = cplx<double>{v[s_lo][col].x, v[s_lo][col].y};
+      h.v[1][col] = cplx<double>{v[s_lo + 1][col].x, v[s_lo + 1][col].y};
       continue;
     }
-    const cplx<double> s0 = ld(0), s1 = ld(1), s2 = ld(2), s3 = ld(3);
+    const cplx<double> s0{v[0][col].x, v[0][col].y}, s1{v[1][col].x, v[1][col].y};
+    const cplx<double> s2{v[2][col].x, v[2][col].y}, s3{v[3][col].x, v[3][col].y};
     if (MU == 0) {
       h.v[0][col] = C > 0 ? s0 + s3 : s0 - s3;
       h.v[1][col] = C > 0 ? s1 + s2 : s1 - s2;
@@ -485,7 +496,7 @@ WL_D void lane_dir_d(const SpinorField<P_DOUBLE>& src, const SiteLinksD& Ls, con
 }
 
 template <bool DAG, int R, class LF, class EPI>
-__global__ void __launch_bounds__(kLaneBlock, 4) hop_lanes_d_kernel(HopArgs<LF, SpinorField<P_DOUBLE>, EPI> A) {
+__global__ void __launch_bounds__(kLaneBlock, WL_LANE_D_MIN_BLOCKS) hop_lanes_d_kernel(HopArgs<LF, SpinorField<P_DOUBLE>, EPI> A) {
   constexpr int S = kLaneBlock / R;
   __shared__ LaneSmemD<R> sm;
   const int tid = threadIdx.x;

@@ -39,7 +39,8 @@ EXPORTS = (
     "wl_gauge_destroy", "wl_apply", "wl_solve", "wl_engine_create", "wl_engine_destroy", "wl_engine_admit",
     "wl_engine_step", "wl_engine_poll", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
     "wl_engine_stream", "wl_engine_time_hop", "wl_kernel_launches", "wl_engine_debug_apply",
-    "wl_apply_schur_normal_noalloc",
+    "wl_apply_schur_normal_noalloc", "wl_gauge_force", "wl_gauge_evolve", "wl_gauge_plaquette_sum",
+    "wl_momentum_kinetic",
 )
 
 
@@ -106,6 +107,10 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wl_kernel_launches": (ctypes.c_int64, []),
         "wl_engine_debug_apply": (i, [vp, i, d, vp, vp]),
         "wl_apply_schur_normal_noalloc": (i, [vp, vp, d, u, vp, vp, i]),
+        "wl_gauge_force": (i, [vp, vp, i, d, vp]),
+        "wl_gauge_evolve": (i, [vp, vp, vp, i, d, vp]),
+        "wl_gauge_plaquette_sum": (i, [vp, vp, i, pd]),
+        "wl_momentum_kinetic": (i, [vp, vp, i, pd]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -253,6 +258,53 @@ class WilsonContext:
         self._check(self.lib.wl_pf_force(self.handle, gauge.handle, _ptr(X), _ptr(Y), float(coef), int(acc),
                                          _ptr(F)))
         return F
+
+    # ------------------------------------------------------------ gauge sector
+    def _links(self, x, name):
+        """Reference-layout BMXYIJ complex128 batch [B, 4, *L, 3, 3] on this device."""
+        x = _c128(x, self.device)
+        if x.numel() % (36 * self.volume) != 0:
+            raise ValueError(f"{name} of {x.numel()} elements does not match [B, 4, {self.lattice_shape}, 3, 3]")
+        return x, x.numel() // (36 * self.volume)
+
+    def gauge_force(self, U, beta: float, out=None):
+        """-(beta/3) TA(U_mu V_mu^dag) per link (su3_ym.py force), U of shape [B, 4, *L, 3, 3]."""
+        import torch
+
+        U, B = self._links(U, "U")
+        if out is None:
+            out = torch.empty_like(U)
+        self._check(self.lib.wl_gauge_force(self.handle, _ptr(U), B, float(beta), _ptr(out)))
+        return out
+
+    def gauge_evolve(self, dt: float, P, U, out=None):
+        """exp(dt P) U per link (su3_ym.py evolve_q with exp_method "expm")."""
+        import torch
+
+        U, B = self._links(U, "U")
+        P, BP = self._links(P, "P")
+        if BP != B:
+            raise ValueError("P and U batch sizes differ")
+        if out is None:
+            out = torch.empty_like(U)
+        self._check(self.lib.wl_gauge_evolve(self.handle, _ptr(P), _ptr(U), B, float(dt), _ptr(out)))
+        return out
+
+    def plaquette_sum(self, U) -> np.ndarray:
+        """sum_{x, mu<nu} Re Tr U_p per configuration (FP64, host array)."""
+        U, B = self._links(U, "U")
+        out = np.zeros(B, dtype=np.float64)
+        self._check(self.lib.wl_gauge_plaquette_sum(self.handle, _ptr(U), B,
+                                                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def kinetic(self, P) -> np.ndarray:
+        """-1/2 sum Re Tr P P per configuration (FP64, host array)."""
+        P, B = self._links(P, "P")
+        out = np.zeros(B, dtype=np.float64)
+        self._check(self.lib.wl_momentum_kinetic(self.handle, _ptr(P), B,
+                                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
 
     def eo_maps(self):
         vh = self.volume // 2

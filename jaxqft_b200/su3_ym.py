@@ -1,7 +1,9 @@
-"""SU(3) pure-gauge pieces on CUDA tensors (torch ops), mirroring
-``jaxqft/models/su3_ym.py`` -- the gauge monomial, momentum refresh, kinetic
-term, exponential drift and link generation that an SU(3) + Wilson-fermion HMC
-needs next to the fermion path.
+"""SU(3) pure-gauge pieces on the device, mirroring ``jaxqft/models/su3_ym.py``
+-- the gauge monomial, momentum refresh, kinetic term, exponential drift and
+link generation that an SU(3) + Wilson-fermion HMC needs next to the fermion
+path.  The plaquette action, staple force, exp(dt P) U drift and kinetic term
+run as sm_100a kernels of libwilson_sm100 (``wl_gauge_*``); momentum refresh
+and link generation use the torch CUDA RNG.
 
 Link layout BMXYIJ ``U[B, mu, Lx, Ly, Lz, Lt, 3, 3]`` (``su3_ym.py:246-249``);
 BXYMIJ is accepted and converted at the boundary.  Everything is complex128
@@ -46,6 +48,8 @@ class SU3YangMills:
     dtype: torch.dtype = torch.complex128
     device: Optional[str] = None
     generator: torch.Generator = field(init=False, repr=False)
+
+    _wl: Optional[object] = field(init=False, default=None, repr=False)
 
     def __post_init__(self):
         self.lattice_shape = tuple(int(v) for v in self.lattice_shape)
@@ -106,46 +110,36 @@ class SU3YangMills:
         return self._sample_algebra(1.0)
 
     # ------------------------------------------------------------------ gauge action / force
+    def _ctx(self):
+        """Geometry context of the CUDA library (periodic; the gauge kernels ignore fermion BCs)."""
+        if self._wl is None:
+            if self.Nd != 4:
+                raise NotImplementedError("the gauge kernels are written for Nd = 4")
+            from .lib import WilsonContext
+
+            self._wl = WilsonContext(self.lattice_shape, bc=(1, 1, 1, 1), device=self.device)
+        return self._wl
+
     def _plaquette_sum(self, U: torch.Tensor) -> torch.Tensor:
-        Ub = self._to_bm(U)
-        s = torch.zeros(Ub.shape[0], dtype=torch.float64, device=Ub.device)
-        for mu in range(self.Nd):
-            Um = Ub[:, mu]
-            for nu in range(mu + 1, self.Nd):
-                Un = Ub[:, nu]
-                p = Um @ torch.roll(Un, -1, dims=1 + mu) @ dagger(torch.roll(Um, -1, dims=1 + nu)) @ dagger(Un)
-                s = s + _trace_re(p).reshape(Ub.shape[0], -1).sum(1)
-        return s
+        s = self._ctx().plaquette_sum(self._to_bm(U))
+        return torch.as_tensor(s, dtype=torch.float64, device=self.device)
 
     def action(self, U: torch.Tensor) -> torch.Tensor:
         """S_g = -(beta/3) sum_p Re Tr U_p (su3_ym.py:264-280)."""
         return -(self.beta / 3.0) * self._plaquette_sum(U)
 
     def force(self, U: torch.Tensor) -> torch.Tensor:
-        """-(beta/3) TA(U_mu staple^dag), for P <- P + dt F (su3_ym.py:296-332)."""
-        Ub = self._to_bm(U)
-        out = []
-        for mu in range(self.Nd):
-            Um = Ub[:, mu]
-            st = torch.zeros_like(Um)
-            for nu in range(self.Nd):
-                if nu == mu:
-                    continue
-                Un = Ub[:, nu]
-                st = st + Un @ torch.roll(Um, -1, dims=1 + nu) @ dagger(torch.roll(Un, -1, dims=1 + mu))
-                Unm = torch.roll(Un, +1, dims=1 + nu)
-                st = st + dagger(Unm) @ torch.roll(Um, +1, dims=1 + nu) @ torch.roll(Unm, -1, dims=1 + mu)
-            out.append(-(self.beta / 3.0) * project_su3_algebra(Um @ dagger(st)))
-        return self._from_bm(torch.stack(out, dim=1))
+        """-(beta/3) TA(U_mu staple^dag), for P <- P + dt F (su3_ym.py:298-327)."""
+        return self._from_bm(self._ctx().gauge_force(self._to_bm(U), self.beta))
 
     def evolve_q(self, dt: float, P: torch.Tensor, Q: torch.Tensor) -> torch.Tensor:
-        """U <- exp(dt P) U (su3_ym.py:352-355)."""
-        return torch.linalg.matrix_exp(dt * P) @ Q
+        """U <- exp(dt P) U (su3_ym.py:349-355, exp_method "expm")."""
+        return self._from_bm(self._ctx().gauge_evolve(dt, self._to_bm(P), self._to_bm(Q)))
 
     def kinetic(self, P: torch.Tensor) -> torch.Tensor:
         """-1/2 sum Re Tr P P (su3_ym.py:362-364)."""
-        trp2 = torch.einsum("...ab,...ba->...", P, P).real
-        return -0.5 * trp2.reshape(P.shape[0], -1).sum(1)
+        k = self._ctx().kinetic(self._to_bm(P))
+        return torch.as_tensor(k, dtype=torch.float64, device=self.device)
 
     def average_plaquette(self, U: torch.Tensor) -> torch.Tensor:
         vol = math.prod(self.lattice_shape)
