@@ -221,6 +221,14 @@ wl_status wl_gauge_plaquette_sum(wl_ctx* ctx, const void* U, int batch, double* 
 /* kin[b] = -1/2 sum Re Tr P P (host array; su3_ym.py:362-364).  Synchronises. */
 wl_status wl_momentum_kinetic(wl_ctx* ctx, const void* P, int batch, double* kin);
 
+/* Measurements -------------------------------------------------------------- */
+/* Pion two-point function of point-source propagator columns
+   (jaxqft/core/measurements.py:375-390): corr[dt] = sum over the timeslice
+   t = source_t + dt (mod Lt) of |S|^2 summed over all `ncol` columns (fermion
+   fields [ncol][Lx][Ly][Lz][Lt][4][3] complex128, device) and their spin and
+   colour.  corr is a host array of Lt doubles.  Synchronises the context stream. */
+wl_status wl_pion_correlator(wl_ctx* ctx, const void* prop, int ncol, int source_t, double* corr);
+
 #ifdef __cplusplus
 }
 #endif

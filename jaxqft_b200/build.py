@@ -17,7 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwilson_sm100.so")
 SOURCES = ["wl_api.cu"]
-HEADERS = ["wl_common.cuh", "wl_hop.cuh", "wl_hop_fast.cuh", "wl_site.cuh", "wl_force.cuh"]
+HEADERS = ["wl_common.cuh", "wl_hop.cuh", "wl_hop_fast.cuh", "wl_site.cuh", "wl_force.cuh", "wl_gauge.cuh",
+           "wl_meas.cuh"]
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC_FLAGS = [

@@ -18,6 +18,7 @@
 #include "../../include/wilson_sm100.h"
 #include "wl_force.cuh"
 #include "wl_gauge.cuh"
+#include "wl_meas.cuh"
 #include "wl_hop_fast.cuh"
 #include "wl_site.cuh"
 
@@ -691,6 +692,27 @@ extern "C" wl_status wl_momentum_kinetic(wl_ctx* ctx, const void* P, int batch, 
   s = check_launch(ctx, "gauge_kinetic_kernel");
   if (s != WL_OK) return s;
   return finish_sums(ctx, batch, nblk, 1.0, kin);
+}
+
+extern "C" wl_status wl_pion_correlator(wl_ctx* ctx, const void* prop, int ncol, int source_t, double* corr) {
+  if (!ctx || !prop || !corr || ncol < 1) WL_FAIL(ctx, WL_ERR_ARG, "null argument or ncol < 1");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  const Geom& g = ctx->g;
+  const int Lt = g.L[3];
+  const int nblk = (g.V / Lt + 127) / 128;
+  wl_status s = ensure_red(ctx, sizeof(double) * ((size_t)Lt * nblk + Lt));
+  if (s != WL_OK) return s;
+  PionArgs A{(const double2*)prop, ncol, g.V, Lt, ctx->red};
+  g_launches++;
+  pion_kernel<<<dim3(nblk, Lt, 1), 128, 0, ctx->stream>>>(A);
+  s = check_launch(ctx, "pion_kernel");
+  if (s != WL_OK) return s;
+  std::vector<double> c(Lt);
+  s = finish_sums(ctx, Lt, nblk, 1.0, c.data());
+  if (s != WL_OK) return s;
+  const int t0 = ((source_t % Lt) + Lt) % Lt;
+  for (int t = 0; t < Lt; ++t) corr[(t - t0 + Lt) % Lt] = c[t];
+  return WL_OK;
 }
 
 // ============================================================== CG engine

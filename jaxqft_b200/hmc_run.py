@@ -34,6 +34,9 @@ def main(argv=None):
     ap.add_argument("--nmd", type=int, default=10)
     ap.add_argument("--tau", type=float, default=1.0)
     ap.add_argument("--ntraj", type=int, default=20)
+    ap.add_argument("--warmup-no-ar", type=int, default=0,
+                    help="initial trajectories without Metropolis accept/reject (thermalisation), as the "
+                         "reference script's --warmup-no-ar")
     ap.add_argument("--integrator", default="minnorm2", choices=["minnorm2", "leapfrog", "forcegrad"])
     ap.add_argument("--monomial", default="unpreconditioned", choices=["unpreconditioned", "eo_preconditioned"])
     ap.add_argument("--precision", default="single", choices=["double", "single", "half"])
@@ -62,6 +65,16 @@ def main(argv=None):
 
     th._solve = counting_solve
     plaq0 = float(th.average_plaquette(U)[0])
+    for k in range(args.warmup_no_ar):
+        # refresh, integrate, always accept (reference hmc_su3_wilson_nf2.py:199-213)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hmc._prepare_trajectory(U)
+        _, U = integ.integrate(th.refreshP(), U)
+        torch.cuda.synchronize()
+        print(json.dumps({"warmup_no_ar": k, "plaquette": float(th.average_plaquette(U)[0]),
+                          "seconds": time.perf_counter() - t0}), flush=True)
+    plaq_meas0 = float(th.average_plaquette(U)[0])
     records = []
     for k in range(args.ntraj):
         iters.clear()
@@ -83,6 +96,7 @@ def main(argv=None):
                "acceptance": hmc.calc_acceptance(), "mean_dH": float(dH.mean()),
                "mean_exp_minus_dH": float(ed.mean()), "err_exp_minus_dH": float(ed.std(ddof=1) / math.sqrt(len(ed)))
                if len(ed) > 1 else float("nan"), "plaquette_start": plaq0,
+               "warmup_no_ar": args.warmup_no_ar, "plaquette_after_warmup": plaq_meas0,
                "plaquette_last": records[-1]["plaquette"] if records else plaq0,
                "seconds_per_traj": float(np.mean([r["seconds"] for r in records])) if records else 0.0}
     print(json.dumps(summary), flush=True)

@@ -40,7 +40,7 @@ EXPORTS = (
     "wl_engine_step", "wl_engine_poll", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
     "wl_engine_stream", "wl_engine_time_hop", "wl_kernel_launches", "wl_engine_debug_apply",
     "wl_apply_schur_normal_noalloc", "wl_gauge_force", "wl_gauge_evolve", "wl_gauge_plaquette_sum",
-    "wl_momentum_kinetic",
+    "wl_momentum_kinetic", "wl_pion_correlator",
 )
 
 
@@ -111,6 +111,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wl_gauge_evolve": (i, [vp, vp, vp, i, d, vp]),
         "wl_gauge_plaquette_sum": (i, [vp, vp, i, pd]),
         "wl_momentum_kinetic": (i, [vp, vp, i, pd]),
+        "wl_pion_correlator": (i, [vp, vp, i, i, pd]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -304,6 +305,18 @@ class WilsonContext:
         out = np.zeros(B, dtype=np.float64)
         self._check(self.lib.wl_momentum_kinetic(self.handle, _ptr(P), B,
                                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def pion_correlator(self, prop, source_t: int) -> np.ndarray:
+        """C(dt), dt = 0..Lt-1, of point-source propagator columns prop [ncol, *L, 4, 3]
+        (measurements.py:375-390): sum of |S|^2 over columns, spin, colour and the timeslice."""
+        prop = _c128(prop, self.device)
+        ncol = prop.numel() // (12 * self.volume)
+        if ncol * 12 * self.volume != prop.numel():
+            raise ValueError(f"propagator of {prop.numel()} elements does not match lattice {self.lattice_shape}")
+        out = np.zeros(self.lattice_shape[3], dtype=np.float64)
+        self._check(self.lib.wl_pion_correlator(self.handle, _ptr(prop), ncol, int(source_t),
+                                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
     def eo_maps(self):

@@ -18,6 +18,11 @@ a normal-equation CG), batched across requests.
   different volumes / gauge fields overlaps on the device.
 * Latency = completion - arrival (queueing included), measured on the host
   clock; each response's solution stays in device memory.
+* A request with ``measure="pion"`` (12 point sources) also gets the pion
+  two-point function (jaxqft/core/measurements.py:375-390) of its propagator:
+  the odd sites are reconstructed from the even solution
+  (x_e = M^-1 eta_e / m0, x_o = -(K x_e)_o / m0, su3_wilson_nf2.py:1325-1335)
+  and contracted on the device.
 """
 
 from __future__ import annotations
@@ -52,6 +57,8 @@ class Request:
     x: Optional[torch.Tensor] = None
     stats: List[dict] = field(default_factory=list)
     pending: int = 0
+    measure: Optional[str] = None      # "pion": contract the 12 point-source columns
+    pion: Optional[np.ndarray] = None  # C(dt), dt = 0..Lt-1, when measured
 
     @property
     def mass(self) -> float:
@@ -224,11 +231,24 @@ class PropagatorServer:
                         req.stats[i] = info
                         req.pending -= 1
                         if req.pending == 0:
+                            if req.measure == "pion":
+                                self._measure_pion(req)
                             req.t_done = time_fn() - t0
                             self.done.append(req)
         if self.device.type == "cuda":
             torch.cuda.synchronize(self.device)
         return self.done
+
+    def _measure_pion(self, req: Request) -> None:
+        if req.kind != "point" or req.nrhs != 12:
+            raise ValueError(f"request {req.rid}: the pion measurement needs the 12 point sources")
+        ctx, gauge = self.ctx[req.volume], self.gauges[(req.volume, req.gauge)]
+        m0 = req.mass + 4.0
+        even = even_mask(req.volume, self.device)
+        xe = req.x * even / m0
+        kxe = ctx.apply("D", gauge, req.mass, xe) - m0 * xe
+        prop = xe - kxe * (1.0 - even) / m0
+        req.pion = ctx.pion_correlator(prop, 0)
 
     def close(self):
         for e in self.engines.values():

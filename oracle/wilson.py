@@ -477,3 +477,32 @@ def algebra_field(rng, shape, batch):
 
 def kappa_to_mass(kappa, r=1.0):
     return 1.0 / (2.0 * kappa) - r * ND
+
+
+# ----------------------------------------------------------------------------- measurements
+def point_source_propagator(U, mass, bc, source, tol=1e-12, maxiter=5000):
+    """S[b, x, s, c, s0, c0] = (D^{-1} delta_{source, s0, c0})(x)_{s c}: one
+    solve_normal(U, apply_Ddag(U, delta)) per (s0, c0), as the iterative
+    backend with the CG solver kind does (jaxqft/core/measurements.py:277-372)."""
+    B = U.shape[0]
+    shape = U.shape[2:6]
+    src = tuple(int(v) % int(n) for v, n in zip(source, shape))
+    prop = np.zeros((B, *shape, 4, 3, 4, 3), dtype=np.complex128)
+    for s0 in range(4):
+        for c0 in range(3):
+            rhs = np.zeros((B, *shape, 4, 3), dtype=np.complex128)
+            rhs[(slice(None), *src, s0, c0)] = 1.0
+            x, _ = solve_normal(U, apply_Ddag(U, rhs, mass, bc), mass, bc, tol, maxiter)
+            prop[..., s0, c0] = x
+    return prop
+
+
+def pion_two_point(prop, source_t):
+    """C(dt) = sum over the timeslice source_t + dt of |S|^2, all batch, spin and
+    colour indices (measurements.py:375-390)."""
+    lt = prop.shape[4]
+    corr = np.zeros(lt)
+    for t in range(lt):
+        slab = prop[:, :, :, :, t]
+        corr[(t - int(source_t)) % lt] = float(np.real(np.sum(np.conj(slab) * slab)))
+    return corr

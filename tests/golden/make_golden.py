@@ -152,6 +152,29 @@ def run_case(R, name, cfg):
           f"cg iters normal={int(out['solve_normal_iters'])} eop={int(out['solve_eop_iters'])}")
 
 
+def run_meas(R):
+    """Point-source propagator and pion correlator through the reference's own
+    measurement code (jaxqft/core/measurements.py:277-390, iterative backend,
+    solver kind "cg": solve_normal(U, apply_Ddag(U, delta)) per column) on a
+    4^4 lattice with an odd-parity source."""
+    import importlib
+
+    meas = importlib.import_module("jaxqft.core.measurements")
+    rng = np.random.default_rng(5)
+    shape, kappa, source = (4, 4, 4, 4), 0.12, (1, 0, 2, 2)
+    mass = 1.0 / (2.0 * kappa) - 4.0
+    th = R.nf2.SU3WilsonNf2(lattice_shape=shape, beta=5.6, batch_size=1, mass=mass, dtype=np.complex128,
+                            fermion_bc=(1, 1, 1, -1), cg_tol=1e-12, cg_maxiter=5000, eo_use_half_spinor=False)
+    U = gen_inputs(rng, shape, 1, 0.3)["U"]
+    prop, _ = meas._full_point_source_propagator(U, th, meas.MeasurementContext(), source, backend="iterative")
+    corr = meas._pion_two_point_from_propagator(np.asarray(prop), source[3])
+    out = dict(U=U, mass=np.float64(mass), shape=np.asarray(shape), source=np.asarray(source),
+               prop=np.asarray(prop), pion=np.asarray(corr))
+    path = os.path.join(HERE, "golden_meas.npz")
+    np.savez(path, **out)
+    print(f"wrote {path}: prop {out['prop'].shape}, pion {out['pion']}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -161,6 +184,7 @@ def main():
     R = load_reference(args.ref)
     for name, cfg in CASES.items():
         run_case(R, name, cfg)
+    run_meas(R)
 
 
 if __name__ == "__main__":

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from oracle import wilson as W
-from tests.conftest import rel
+from tests.conftest import load_golden, rel
 
 TOL = 1e-13
 
@@ -141,3 +141,11 @@ def test_gamma5_hermiticity_and_adjoint():
     a = W.vdot(chi, W.apply_D(U, psi, 0.05, bc))
     b = W.vdot(W.apply_Ddag(U, chi, 0.05, bc), psi)
     assert abs(a - b) / abs(a) < 1e-14
+
+
+def test_point_propagator_and_pion_match_reference():
+    """Oracle vs the reference's own measurement code (golden_meas.npz)."""
+    g = load_golden("meas")
+    prop = W.point_source_propagator(g["U"], float(g["mass"]), (1, 1, 1, -1), tuple(g["source"]))
+    assert rel(prop, g["prop"]) < 1e-10
+    assert np.allclose(W.pion_two_point(g["prop"], int(g["source"][3])), g["pion"], rtol=1e-13, atol=0)
