@@ -51,6 +51,58 @@ def _chrono_predict(history: List[torch.Tensor], mode: str, max_hist: int) -> Op
     return x0
 
 
+def _chrono_predict_mre(xs: List[torch.Tensor], ys: List[torch.Tensor], target: torch.Tensor,
+                        reg: float = 1e-12) -> Optional[torch.Tensor]:
+    """Minimal-residual extrapolation (su3_wilson_nf2.py:114-194): with history
+    pairs (x_i, y_i = L x_i), minimise ||target - sum_i c_i y_i|| over c with
+    older entries damped by exp(-0.35 age), Tikhonov regularisation reg*tr(G)/n,
+    and the reference's safeguards (coefficient bounds, trust-region blend
+    towards x_last, norm growth limit, and acceptance only if the subspace
+    residual beats the latest image by 3 %).  Inner products run on the device;
+    the n x n solve on the host, as in the reference."""
+    if not xs or not ys:
+        return None
+    if len(xs) == 1:
+        return xs[-1]
+    n = len(xs)
+    w = np.asarray([math.exp(-0.35 * float((n - 1) - i)) for i in range(n)])
+    G = np.zeros((n, n), dtype=np.complex128)
+    g = np.zeros((n,), dtype=np.complex128)
+    for i in range(n):
+        g[i] = w[i] * complex(_vdot(ys[i], target))
+        for j in range(i, n):
+            gij = w[i] * w[j] * complex(_vdot(ys[i], ys[j]))
+            G[i, j] = gij
+            G[j, i] = np.conj(gij)
+    lam = float(reg) * max(1.0, abs(float(np.trace(G).real)) / max(1, n))
+    Greg = G + lam * np.eye(n, dtype=np.complex128)
+    try:
+        c = np.linalg.solve(Greg, g)
+    except np.linalg.LinAlgError:
+        c, *_ = np.linalg.lstsq(Greg, g, rcond=None)
+    c = c * w
+    if not np.all(np.isfinite(c)):
+        return xs[-1]
+    cmax, cl1 = float(np.max(np.abs(c))), float(np.sum(np.abs(c)))
+    if cmax > 2.0 or cl1 > 3.0:
+        return xs[-1]
+    x0 = torch.zeros_like(xs[-1])
+    for ci, xi in zip(c, xs):
+        x0 = x0 + complex(ci) * xi
+    beta = 1.0 / max(1.0, cl1)
+    x0 = beta * x0 + (1.0 - beta) * xs[-1]
+    n_last, n_x0 = float(_field_norm(xs[-1])), float(_field_norm(x0))
+    if not math.isfinite(n_x0) or (n_last > 0.0 and n_x0 > 5.0 * n_last):
+        return xs[-1]
+    y_comb = torch.zeros_like(ys[-1])
+    for ci, yi in zip(c, ys):
+        y_comb = y_comb + complex(ci) * yi
+    r_mre, r_last = float(_field_norm(target - y_comb)), float(_field_norm(target - ys[-1]))
+    if not (math.isfinite(r_mre) and math.isfinite(r_last)) or r_mre >= 0.97 * r_last:
+        return xs[-1]
+    return x0
+
+
 @dataclass
 class GaugeActionMonomial:
     """Plaquette monomial (su3_wilson_nf2.py:197-214)."""
@@ -82,26 +134,40 @@ class _PFBase:
     eta: Optional[torch.Tensor] = field(default=None, init=False, repr=False)
     phi: Optional[torch.Tensor] = field(default=None, init=False, repr=False)
     _hist: List[torch.Tensor] = field(default_factory=list, init=False, repr=False)
+    _img: List[Optional[torch.Tensor]] = field(default_factory=list, init=False, repr=False)
 
     def clear(self) -> None:
         self.eta = None
         self.phi = None
         self._hist = []
+        self._img = []
 
     def clear_solver_guess(self) -> None:
         self._hist = []
+        self._img = []
 
     def _guess(self):
+        """Initial guess from the solve history (su3_wilson_nf2.py:254-284)."""
         m = self.model
         if not m.use_solver_guess:
             return None
-        mode = "poly" if m.solver_guess_mode in ("poly", "mre") else "last"
-        return _chrono_predict(self._hist, mode, m.solver_guess_history)
+        keep = max(1, int(m.solver_guess_history))
+        mode = str(m.solver_guess_mode).lower()
+        if mode == "mre" and self.eta is not None:
+            pairs = [(x, y) for x, y in zip(self._hist[-keep:], self._img[-keep:])
+                     if y is not None and y.shape == self.eta.shape]
+            if pairs:
+                x0 = _chrono_predict_mre([p[0] for p in pairs], [p[1] for p in pairs], self.eta)
+                if x0 is not None:
+                    return x0
+            mode = "poly"  # no images / no eta (OU refresh): polynomial fallback
+        return _chrono_predict(self._hist, "poly" if mode == "poly" else "last", keep)
 
-    def _remember(self, x):
+    def _remember(self, x, y=None):
         if self.model.use_solver_guess:
-            self._hist.append(x)
-            self._hist = self._hist[-max(1, int(self.model.solver_guess_history)):]
+            keep = max(1, int(self.model.solver_guess_history))
+            self._hist = (self._hist + [x])[-keep:]
+            self._img = (self._img + [y])[-keep:]
 
     def _ou_coeffs(self, traj_length):
         c1 = math.exp(-float(self.gamma) * float(traj_length))
@@ -135,6 +201,7 @@ class WilsonNf2PseudofermionMonomial(_PFBase):
         else:
             raise ValueError(f"Unknown pseudofermion refresh mode: {self.refresh_mode}")
         self._hist = []
+        self._img = []
 
     def action(self, q):
         if self.phi is None:
@@ -146,8 +213,8 @@ class WilsonNf2PseudofermionMonomial(_PFBase):
         m = self.model
         x0 = self._guess()
         x = m.solve_normal(q, phi) if x0 is None else m.solve_normal_with_guess(q, phi, x0)
-        self._remember(x)
         y = m.apply_D(q, x)
+        self._remember(x, y)
         return m.pseudofermion_force_from_solution(q, x, y)
 
 
@@ -173,6 +240,7 @@ class WilsonNf2EOPreconditionedMonomial(_PFBase):
         else:
             raise ValueError(f"Unknown pseudofermion refresh mode: {self.refresh_mode}")
         self._hist = []
+        self._img = []
 
     def action(self, q):
         if self.phi is None:
@@ -184,8 +252,8 @@ class WilsonNf2EOPreconditionedMonomial(_PFBase):
         m = self.model
         x0 = self._guess()
         xe = m.solve_eop_even_normal(q, phi) if x0 is None else m.solve_eop_even_normal_with_guess(q, phi, x0)
-        self._remember(xe)
         ye = m.apply_eo_schur_even(q, xe, normalized=True)
+        self._remember(xe, ye)
         return m.eop_pseudofermion_force_from_solution(q, xe, ye)
 
 

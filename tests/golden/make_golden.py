@@ -175,6 +175,68 @@ def run_meas(R):
     print(f"wrote {path}: prop {out['prop'].shape}, pion {out['pion']}")
 
 
+def run_chrono(R):
+    """Chronological initial guesses through the reference's own predictors
+    (jaxqft/models/su3_wilson_nf2.py:85-194) on synthetic histories: y_i = A x_i
+    for a fixed well-conditioned A, target = A (a smooth extrapolation of the
+    x_i) + small noise, so that the MRE guess is accepted; a second target far
+    from the image span exercises the fallback to the last solution."""
+    rng = np.random.default_rng(9)
+    shape = (1, 2, 2, 2, 2, 4, 3)
+    n = int(np.prod(shape))
+    A = np.eye(n) + 0.3 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / np.sqrt(n)
+
+    def field():
+        return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) / np.sqrt(2.0)
+
+    base, drift = field(), field()
+    xs = [base + 0.1 * k * drift + 0.01 * field() for k in range(4)]
+    ys = [(A @ x.reshape(-1)).reshape(shape) for x in xs]
+    x_next = base + 0.4 * drift
+    target = (A @ x_next.reshape(-1)).reshape(shape) + 1e-3 * field()
+    far = 10.0 * field()
+    out = dict(xs=np.stack(xs), ys=np.stack(ys), target=target, far=far)
+    out["mre"] = np.asarray(R.nf2._chrono_predict_mre(xs, ys, target, 4))
+    out["mre_far"] = np.asarray(R.nf2._chrono_predict_mre(xs, ys, far, 4))
+    out["poly"] = np.asarray(R.nf2._chrono_predict_from_history(xs, "poly", 4))
+    out["poly3"] = np.asarray(R.nf2._chrono_predict_from_history(xs, "poly", 3))
+    out["last"] = np.asarray(R.nf2._chrono_predict_from_history(xs, "last", 4))
+    path = os.path.join(HERE, "golden_chrono.npz")
+    np.savez(path, **out)
+    print(f"wrote {path}: mre differs from last by {np.linalg.norm(out['mre'] - out['last']):.3e}, "
+          f"far fallback diff {np.linalg.norm(out['mre_far'] - out['last']):.3e}")
+
+
+def run_lime(ref_root):
+    """SciDAC LIME files written by jaxqft_b200.lime (gauge in D and F precision,
+    one Dirac fermion) and decoded by the reference's own reader
+    (jaxqft/io/lime.py decode_scidac_gauge / decode_scidac_pseudofermion)."""
+    import importlib.util
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from jaxqft_b200 import lime as ours
+
+    spec = importlib.util.spec_from_file_location("ref_lime", os.path.join(ref_root, "jaxqft", "io", "lime.py"))
+    ref = importlib.util.module_from_spec(spec)
+    sys.modules["ref_lime"] = ref
+    spec.loader.exec_module(ref)
+    rng = np.random.default_rng(13)
+    shape = (2, 4, 4, 6)
+    U = gen_inputs(rng, shape, 1, 0.5)["U"][0]
+    psi = (rng.standard_normal((*shape, 4, 3)) + 1j * rng.standard_normal((*shape, 4, 3))) / np.sqrt(2.0)
+    out = {}
+    for p in ("D", "F"):
+        fn = os.path.join(HERE, f"gauge_{p}.lime")
+        ours.save_gauge(fn, U, precision=p)
+        out[f"U_{p}"] = ref.decode_scidac_gauge(fn)
+    fn = os.path.join(HERE, "fermion_D.lime")
+    ours.save_fermion(fn, psi)
+    out["psi"], _ = ref.decode_scidac_pseudofermion(fn)
+    out["U"], out["psi_in"] = U, psi
+    np.savez(os.path.join(HERE, "golden_lime.npz"), **out)
+    print("wrote LIME golden files", {k: v.shape for k, v in out.items()})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -185,6 +247,8 @@ def main():
     for name, cfg in CASES.items():
         run_case(R, name, cfg)
     run_meas(R)
+    run_chrono(R)
+    run_lime(args.ref)
 
 
 if __name__ == "__main__":

@@ -80,3 +80,19 @@ def test_theory_mirror_layouts(fields, layout):
     assert rel(F.cpu().numpy(), W.gauge_force(U, 5.6)) < 1e-13
     assert rel(U2.cpu().numpy(), W.evolve_q(0.3, P, U)) < 1e-13
     assert np.allclose(th.kinetic(Pt).cpu().numpy(), W.kinetic(P), rtol=1e-13)
+
+
+def test_lime_configuration_on_device():
+    """A SciDAC LIME configuration read straight into device memory feeds the
+    gauge kernels: plaquette of the file = oracle plaquette of the stored links."""
+    import os
+
+    from jaxqft_b200 import lime
+    from tests.conftest import GOLDEN, load_golden
+
+    g = load_golden("lime")
+    U = lime.load_gauge(os.path.join(GOLDEN, "gauge_D.lime"))
+    assert U.is_cuda and U.dtype == torch.complex128
+    shape = tuple(U.shape[2:6])
+    ctx = WilsonContext(shape, bc=(1, 1, 1, 1))
+    assert np.allclose(ctx.plaquette_sum(U), W.plaquette_sum(g["U_D"]), rtol=1e-13, atol=0)
