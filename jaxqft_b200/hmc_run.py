@@ -34,6 +34,8 @@ def main(argv=None):
     ap.add_argument("--nmd", type=int, default=10)
     ap.add_argument("--tau", type=float, default=1.0)
     ap.add_argument("--ntraj", type=int, default=20)
+    ap.add_argument("--load", default=None, help="start from a SciDAC LIME gauge configuration")
+    ap.add_argument("--save", default=None, help="write the final configuration as SciDAC LIME")
     ap.add_argument("--warmup-no-ar", type=int, default=0,
                     help="initial trajectories without Metropolis accept/reject (thermalisation), as the "
                          "reference script's --warmup-no-ar")
@@ -50,7 +52,14 @@ def main(argv=None):
                       fermion_bc=(1, 1, 1, -1), cg_tol=args.cg_tol, cg_maxiter=args.cg_maxiter,
                       fermion_monomial_kind=args.monomial, pseudofermion_force_mode="analytic",
                       solver_precision=args.precision, action_cg_tol=args.action_tol, seed=args.seed)
-    U = th.hot_start(scale=args.start_scale)
+    if args.load:
+        from . import lime
+
+        U = lime.load_gauge(args.load, device=th.device)
+        if tuple(U.shape[2:6]) != shape:
+            raise ValueError(f"{args.load}: lattice {tuple(U.shape[2:6])} differs from --shape {shape}")
+    else:
+        U = th.hot_start(scale=args.start_scale)
     cls = {"minnorm2": MinNorm2, "leapfrog": Leapfrog, "forcegrad": ForceGradient}[args.integrator]
     integ = cls(th.force, th.evolve_q, args.nmd, args.tau)
     hmc = HMC(th, integ, verbose=False, seed=args.seed + 1)
@@ -100,6 +109,10 @@ def main(argv=None):
                "plaquette_last": records[-1]["plaquette"] if records else plaq0,
                "seconds_per_traj": float(np.mean([r["seconds"] for r in records])) if records else 0.0}
     print(json.dumps(summary), flush=True)
+    if args.save:
+        from . import lime
+
+        lime.save_gauge(args.save, U)
     return summary
 
 
