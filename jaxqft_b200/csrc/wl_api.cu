@@ -19,6 +19,7 @@
 #include "wl_force.cuh"
 #include "wl_gauge.cuh"
 #include "wl_meas.cuh"
+#include "wl_rowhop.cuh"
 #include "wl_hop_fast.cuh"
 #include "wl_site.cuh"
 
@@ -36,6 +37,8 @@ struct wl_ctx {
   // scratch for the gauge-sector reductions (block partials + per-batch results)
   double* red = nullptr;
   size_t red_bytes = 0;
+  int* dev_err = nullptr;  // set by kernels whose bounded waits ran out (read at wl_ctx_synchronize)
+  int sm_count = 0;
 };
 
 struct wl_gauge {
@@ -329,6 +332,12 @@ extern "C" wl_status wl_ctx_create(const wl_geometry* geom, int device, wl_ctx**
     g.ph_im[mu] = geom->bc_im[mu];
     g.ph_on[mu] = (std::fabs(geom->bc_re[mu] - 1.0) > 1e-12 || std::fabs(geom->bc_im[mu]) > 1e-12) ? 1 : 0;
   }
+  if (cudaMalloc(&c->dev_err, sizeof(int)) != cudaSuccess || cudaMemset(c->dev_err, 0, sizeof(int)) != cudaSuccess ||
+      cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+    if (c->dev_err) cudaFree(c->dev_err);
+    delete c;
+    WL_FAIL(nullptr, WL_ERR_CUDA, "context set-up failed");
+  }
   *out = c;
   return WL_OK;
 }
@@ -339,6 +348,7 @@ extern "C" void wl_ctx_destroy(wl_ctx* ctx) {
   wl_release_solve_cache(ctx);
   if (ctx->tmp) cudaFree(ctx->tmp);
   if (ctx->red) cudaFree(ctx->red);
+  if (ctx->dev_err) cudaFree(ctx->dev_err);
   delete ctx;
 }
 
@@ -353,6 +363,14 @@ extern "C" wl_status wl_ctx_set_stream(wl_ctx* ctx, void* stream) {
 extern "C" wl_status wl_ctx_synchronize(wl_ctx* ctx) {
   if (!ctx) WL_FAIL(nullptr, WL_ERR_ARG, "null context");
   WL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->dev_err) {
+    int e = 0;
+    WL_CUDA(ctx, cudaMemcpy(&e, ctx->dev_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+      WL_CUDA(ctx, cudaMemset(ctx->dev_err, 0, sizeof(int)));
+      WL_FAIL(ctx, WL_ERR_TIMEOUT, "a bounded device wait ran out (row-staged operator); its output is invalid");
+    }
+  }
   return WL_OK;
 }
 
@@ -499,9 +517,54 @@ static wl_status ensure_tmp(wl_ctx* ctx, size_t bytes) {
 }
 
 // out(target parities) = a*self + b*hop(in); npar = 2 for both parities, else target parity0 only
+static bool row_hop_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("WL_ROW_HOP");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// Row-staged (TMA bulk copy) FP64 hop for the reference layout; false if the
+// lattice does not fit its shared-memory stages.
+template <bool DAG>
+static bool row_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const void* self, double a, double b,
+                    int nrhs, int pmask) {
+  const Geom& g = ctx->g;
+  const int Lt = g.L[3];
+  if (!row_hop_enabled() || Lt > kRowMaxLt) return false;
+  RowHopArgs A{};
+  A.g = g;
+  A.U = G->ref_copy;
+  A.in = (const double2*)in;
+  A.out = (double2*)out;
+  A.self = (const double2*)self;
+  A.a = a;
+  A.b = b;
+  A.nrhs = nrhs;
+  A.pmask = pmask;
+  A.err = ctx->dev_err;
+  const int threads = ((3 * Lt + 31) / 32) * 32;
+  const size_t smem = 128 + (size_t)kRowBufs * row_stage_bytes(Lt);
+  int per_sm = 0;
+  if (cudaFuncSetAttribute(row_hop_kernel<DAG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, row_hop_kernel<DAG>, threads, smem) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();  // fall back to the thread-per-site kernel; clear the error this left
+    return false;
+  }
+  const long long items = (long long)(g.V / Lt) * nrhs;
+  const int blocks = (int)std::min<long long>(items, (long long)per_sm * ctx->sm_count);
+  g_launches++;
+  row_hop_kernel<DAG><<<blocks, threads, smem, ctx->stream>>>(A);
+  return true;
+}
+
 template <bool DAG>
 static void ref_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const void* self, double a, double b,
                     int nrhs, int parity0, int npar) {
+  if (row_hop<DAG>(ctx, G, in, out, self, a, b, nrhs, npar == 2 ? 3 : (1 << parity0))) return;
   RefHopArgs A = ref_args(ctx, G, in, out, self, a, b, nrhs, parity0);
   Tune t;
   t.nr = 1;
