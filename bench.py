@@ -250,6 +250,27 @@ def run_ours(args):
     achieved = hop_bytes / (hop_ms * 1e-3) / 1e9
     traffic = profile_traffic(f"hop_h12_half_nrhs{NRHS}_{'x'.join(map(str, SHAPE))}")
 
+    # ---- the drop-in FP64 Dslash (reference layout, apply_D), 1 RHS: GB/s against the same peak
+    psi1 = eta[NRHS - 1:NRHS].contiguous()
+    dout = torch.empty_like(psi1)
+    for _ in range(3):
+        ctx.apply("D", gauge, MASS, psi1, out=dout)
+    cur0 = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(cur0)
+    for _ in range(20):
+        ctx.apply("D", gauge, MASS, psi1, out=dout)
+    e1.record(cur0)
+    e1.synchronize()
+    ctx.synchronize()
+    d_ms = e0.elapsed_time(e1) / 20
+    d_bytes = float(np.prod(SHAPE)) * (4 * 144 + 2 * 192)  # 4 links + in/out spinor per site (FP64)
+    dslash = {"kernel": "D = m0 - hop/2, reference layout, FP64, 1 RHS (row-staged TMA bulk copies)",
+              "ms_per_launch": d_ms, "algorithmic_bytes_per_launch": d_bytes,
+              "achieved": d_bytes / (d_ms * 1e-3) / 1e9, "unit": "GB/s"}
+    dslash["frac"] = dslash["achieved"] / peaks()[0]
+    del psi1, dout
+
     # ---- e2e through the public API from pinned host buffers
     e2e = None
     if rank == 0 or True:
@@ -311,6 +332,7 @@ def run_ours(args):
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": hop_bytes,
                          "ms_per_launch": hop_ms, "traffic": traffic},
+            "dslash_fp64": dslash,
             "e2e": e2e,
             "serve": serve,
             "gpu_launches": int(launches),
@@ -420,6 +442,41 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_dslash(args):
+    """Profiling driver for the drop-in FP64 Dslash (reference layout, 1 RHS):
+    3 warm-up applications, then `--profile-dslash` applications of D between
+    cudaProfilerStart/Stop."""
+    import torch
+
+    from jaxqft_b200 import lib as L
+
+    global SHAPE
+    SHAPE = tuple(int(v) for v in args.shape.split(","))
+    dev = torch.device("cuda", 0)
+    ctx = L.WilsonContext(SHAPE, bc=BC, device=dev)
+    U, eta = make_inputs(torch, dev, seed=0)
+    gauge = ctx.gauge(U)
+    psi = eta[NRHS - 1:NRHS].contiguous()
+    del U, eta
+    out = torch.empty_like(psi)
+    for _ in range(3):
+        ctx.apply("D", gauge, MASS, psi, out=out)
+    ctx.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.profile_dslash):
+        ctx.apply("D", gauge, MASS, psi, out=out)
+    e1.record()
+    e1.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
+    ctx.synchronize()
+    ms = e0.elapsed_time(e1) / args.profile_dslash
+    byts = float(np.prod(SHAPE)) * 960.0
+    print(json.dumps({"profile": "FP64 D, reference layout, 1 RHS", "shape": SHAPE, "ms": ms,
+                      "GBps": byts / ms / 1e6}), flush=True)
+
+
 def run_profile(args):
     """Profiling driver: a fixed number of batched CG iterations of the same
     solver, bracketed by cudaProfilerStart/Stop so that
@@ -478,10 +535,14 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=153,
                     help="FP64 CG iterations to 1e-10 on this system: plain FP64 CG needs 152-154 on each of the "
                          "16 RHS (measured with --fp64-all)")
+    ap.add_argument("--profile-dslash", type=int, default=0,
+                    help="profiling driver: this many FP64 reference-layout D applications (on --shape)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.profile_iters > 0:
+    if args.profile_dslash > 0:
+        run_profile_dslash(args)
+    elif args.profile_iters > 0:
         run_profile(args)
     elif args.impl == "reference":
         run_reference(args)
