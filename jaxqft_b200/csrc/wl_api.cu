@@ -13,6 +13,8 @@
 #include <string>
 #include <tuple>
 #include <type_traits>
+
+#include <cudaTypedefs.h>
 #include <vector>
 
 #include "../../include/wilson_sm100.h"
@@ -525,14 +527,41 @@ static bool row_hop_enabled() {
   return on;
 }
 
-// Row-staged (TMA bulk copy) FP64 hop for the reference layout; false if the
-// lattice does not fit its shared-memory stages.
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link needed)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// Row-staged (TMA) FP64 hop for the reference layout; false if the lattice does
+// not fit its shared-memory stages or the tensor map cannot be built.
 template <bool DAG>
 static bool row_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const void* self, double a, double b,
                     int nrhs, int pmask) {
   const Geom& g = ctx->g;
   const int Lt = g.L[3];
   if (!row_hop_enabled() || Lt > kRowMaxLt) return false;
+  const long long lines = (long long)nrhs * g.V * 3 / 2;  // the fields as 128-byte lines
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || lines >= (1LL << 31) || ((uintptr_t)in & 15)) return false;
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {16, (cuuint64_t)lines};
+  const cuuint64_t strides[1] = {128};
+  const cuuint32_t box[2] = {16, (cuuint32_t)(Lt * 3 / 2)};
+  const cuuint32_t estr[2] = {1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(in), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
   RowHopArgs A{};
   A.g = g;
   A.U = G->ref_copy;
@@ -545,7 +574,7 @@ static bool row_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const v
   A.pmask = pmask;
   A.err = ctx->dev_err;
   const int threads = ((3 * Lt + 31) / 32) * 32;
-  const size_t smem = 128 + (size_t)kRowBufs * row_stage_bytes(Lt);
+  const size_t smem = 128 + 1024 + (size_t)kRowBufs * row_stage_bytes(Lt);
   int per_sm = 0;
   if (cudaFuncSetAttribute(row_hop_kernel<DAG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
           cudaSuccess ||
@@ -557,7 +586,7 @@ static bool row_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const v
   const long long items = (long long)(g.V / Lt) * nrhs;
   const int blocks = (int)std::min<long long>(items, (long long)per_sm * ctx->sm_count);
   g_launches++;
-  row_hop_kernel<DAG><<<blocks, threads, smem, ctx->stream>>>(A);
+  row_hop_kernel<DAG><<<blocks, threads, smem, ctx->stream>>>(map, A);
   return true;
 }
 

@@ -22,6 +22,8 @@
 // backward hop into x_mu = 0.  Waits on the mbarriers are bounded; on time-out
 // the block records an error flag and stops.
 #pragma once
+#include <cuda.h>  // CUtensorMap (the map itself is encoded on the host through the driver entry point)
+
 #include "wl_hop.cuh"
 
 namespace wl {
@@ -56,6 +58,27 @@ WL_D void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long lon
                "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
+// 2D tensor-map global -> shared copy (box defined by the map), completing on `bar` (no multicast)
+WL_D void tma_g2s_2d(void* dst, const CUtensorMap* map, int c0, int c1, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// The spinor rows are copied with the TMA 128-byte swizzle: viewed as 128-byte
+// lines, the 16-byte chunk j of line r lands at chunk j ^ (r mod 8) (buffer
+// 1024-byte aligned).  This spreads the components that the sites of one warp
+// read at the same time (192-byte site stride: every other site on the same
+// banks otherwise) over the bank groups.
+WL_D const double2* swz_psi(const unsigned char* chunk, int site, int comp) {
+  const unsigned o = (unsigned)site * 192u + (unsigned)comp * 16u;
+  const unsigned line = o >> 7;
+  const unsigned j = ((o >> 4) & 7u) ^ (line & 7u);
+  return reinterpret_cast<const double2*>(chunk + (line << 7) + (j << 4));
+}
+
 // order this thread's earlier generic-proxy shared-memory accesses before later async-proxy ones
 WL_D void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
@@ -64,8 +87,9 @@ WL_D void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta
 #endif
 constexpr int kRowBufs = WL_ROW_BUFS;  // stage buffers per block (kRowBufs - 1 stages prefetched)
 constexpr int kRowStages = 4;          // stages per row
-// largest Lt whose kRowBufs stages (672*Lt bytes each) fit in shared memory, and 3*Lt threads in a block
-constexpr int kRowMaxLt = (225 * 1024) / (672 * kRowBufs) < 148 ? (225 * 1024) / (672 * kRowBufs) : 148;
+// largest Lt whose kRowBufs stages (~672*Lt bytes each, padded) fit in shared memory, 3*Lt threads in a
+// block, and a psi row of 1.5*Lt lines in one tensor-map box (<= 256)
+constexpr int kRowMaxLt = (220 * 1024) / (672 * kRowBufs) < 148 ? (220 * 1024) / (672 * kRowBufs) : 148;
 constexpr long long kRowWaitLimit = 1LL << 24;  // try_wait rounds before a wait is declared lost
 
 struct RowHopArgs {
@@ -84,7 +108,9 @@ struct RowStage {
   int item, mu;
 };
 
-WL_HD size_t row_stage_bytes(int Lt) { return (size_t)672 * Lt; }
+// psi chunks padded to 1024 bytes (swizzle atom), link chunks after them
+WL_HD size_t row_psi_pad(int Lt) { return (((size_t)192 * Lt + 1023) / 1024) * 1024; }
+WL_HD size_t row_stage_bytes(int Lt) { return ((2 * row_psi_pad(Lt) + (size_t)288 * Lt + 1023) / 1024) * 1024; }
 
 WL_D RowStage row_stage_of(int k) {
   RowStage s;
@@ -94,18 +120,22 @@ WL_D RowStage row_stage_of(int k) {
   return s;
 }
 
-// buffer layout of a stage: [psi A | psi B | U fwd | U bwd], chunks of 192*Lt / 144*Lt bytes
-WL_D void row_stage_issue(const RowHopArgs& A, const RowStage& st, unsigned char* buf, unsigned long long* bar) {
+// buffer layout of a stage: [psi A | psi B | U fwd | U bwd]: swizzled psi rows (tensor map over the
+// field viewed as 128-byte lines, box = one row = 1.5*Lt lines) padded to 1024 bytes, then 144*Lt-byte link rows
+WL_D void row_stage_issue(const RowHopArgs& A, const CUtensorMap* psimap, const RowStage& st, unsigned char* buf,
+                          unsigned long long* bar) {
   const Geom& g = A.g;
   const int Lt = g.L[3];
   const int nrows = g.V / Lt;
   const int rhs = st.item / nrows, row = st.item - rhs * nrows;
-  const size_t sp = (size_t)192 * Lt, lk = (size_t)144 * Lt;
-  const double2* in = A.in + (size_t)rhs * g.V * 12;
+  const size_t spad = row_psi_pad(Lt), lk = (size_t)144 * Lt;
+  const unsigned sp = 192u * (unsigned)Lt;
+  const int line0 = (int)(((long long)rhs * g.V) * 3 / 2);  // first 128-byte line of this RHS
+  const int lpr = Lt * 3 / 2;                               // lines per row (Lt even)
   if (st.mu == 3) {
     mbar_expect_tx(bar, (unsigned)(sp + lk));
-    bulk_g2s(buf, in + (size_t)row * Lt * 12, (unsigned)sp, bar);
-    bulk_g2s(buf + 2 * sp, A.U + ((size_t)3 * g.V + (size_t)row * Lt) * 9, (unsigned)lk, bar);
+    tma_g2s_2d(buf, psimap, 0, line0 + row * lpr, bar);
+    bulk_g2s(buf + 2 * spad, A.U + ((size_t)3 * g.V + (size_t)row * Lt) * 9, (unsigned)lk, bar);
     return;
   }
   // row = (x*Ly + y)*Lz + z ; neighbour rows along mu with periodic wrap
@@ -115,21 +145,22 @@ WL_D void row_stage_issue(const RowHopArgs& A, const RowStage& st, unsigned char
   const int rp = row + (xm == Lm - 1 ? -(Lm - 1) * stride : stride);
   const int rm = row + (xm == 0 ? (Lm - 1) * stride : -stride);
   mbar_expect_tx(bar, (unsigned)(2 * sp + 2 * lk));
-  bulk_g2s(buf, in + (size_t)rp * Lt * 12, (unsigned)sp, bar);
-  bulk_g2s(buf + sp, in + (size_t)rm * Lt * 12, (unsigned)sp, bar);
-  bulk_g2s(buf + 2 * sp, A.U + ((size_t)st.mu * g.V + (size_t)row * Lt) * 9, (unsigned)lk, bar);
-  bulk_g2s(buf + 2 * sp + lk, A.U + ((size_t)st.mu * g.V + (size_t)rm * Lt) * 9, (unsigned)lk, bar);
+  tma_g2s_2d(buf, psimap, 0, line0 + rp * lpr, bar);
+  tma_g2s_2d(buf + spad, psimap, 0, line0 + rm * lpr, bar);
+  bulk_g2s(buf + 2 * spad, A.U + ((size_t)st.mu * g.V + (size_t)row * Lt) * 9, (unsigned)lk, bar);
+  bulk_g2s(buf + 2 * spad + lk, A.U + ((size_t)st.mu * g.V + (size_t)rm * Lt) * 9, (unsigned)lk, bar);
 }
 
 // One direction for thread (site t, colour a): acc[s] += [(1 + C g_mu) W psi]_s,a with W = ph*U
 // (forward) or (ph*U)^dag (backward, DAGU), psi and the link read from shared memory.
 template <int MU, int C, bool DAGU>
-WL_D void row_dir(const double2* psi, const double2* u, int a, bool ph, const Geom& g, cplx<double> (&acc)[4]) {
+WL_D void row_dir(const unsigned char* chunk, int site, const double2* u, int a, bool ph, const Geom& g,
+                  cplx<double> (&acc)[4]) {
   Half<double> h;
 #pragma unroll
   for (int col = 0; col < 3; ++col) {
     auto ld = [&](int sp) {
-      const double2 v = psi[sp * 3 + col];
+      const double2 v = *swz_psi(chunk, site, sp * 3 + col);
       return cplx<double>{v.x, v.y};
     };
     if (MU == 3) {
@@ -197,21 +228,21 @@ WL_D void row_stage_compute(const RowHopArgs& A, const unsigned char* buf, int r
   constexpr int CB = -CF;
   const Geom& g = A.g;
   const int Lt = g.L[3];
-  const size_t sp = (size_t)192 * Lt, lk = (size_t)144 * Lt;
-  const double2* psiA = reinterpret_cast<const double2*>(buf);
-  const double2* psiB = reinterpret_cast<const double2*>(buf + sp);
-  const double2* Uf = reinterpret_cast<const double2*>(buf + 2 * sp);
-  const double2* Ub = reinterpret_cast<const double2*>(buf + 2 * sp + lk);
+  const size_t spad = row_psi_pad(Lt), lk = (size_t)144 * Lt;
+  const unsigned char* psiA = buf;
+  const unsigned char* psiB = buf + spad;
+  const double2* Uf = reinterpret_cast<const double2*>(buf + 2 * spad);
+  const double2* Ub = reinterpret_cast<const double2*>(buf + 2 * spad + lk);
   if (MU == 3) {
     const int tp = t == Lt - 1 ? 0 : t + 1, tm = t == 0 ? Lt - 1 : t - 1;
     const bool on = g.ph_on[3] != 0;
-    row_dir<3, CF, false>(psiA + tp * 12, Uf + t * 9, a, on && t == Lt - 1, g, acc);
-    row_dir<3, CB, true>(psiA + tm * 12, Uf + tm * 9, a, on && t == 0, g, acc);
+    row_dir<3, CF, false>(psiA, tp, Uf + t * 9, a, on && t == Lt - 1, g, acc);
+    row_dir<3, CB, true>(psiA, tm, Uf + tm * 9, a, on && t == 0, g, acc);
   } else {
     const int xm = (row / g.strideRow[MU]) % g.L[MU];
     const bool on = g.ph_on[MU] != 0;
-    row_dir<MU, CF, false>(psiA + t * 12, Uf + t * 9, a, on && xm == g.L[MU] - 1, g, acc);
-    row_dir<MU, CB, true>(psiB + t * 12, Ub + t * 9, a, on && xm == 0, g, acc);
+    row_dir<MU, CF, false>(psiA, t, Uf + t * 9, a, on && xm == g.L[MU] - 1, g, acc);
+    row_dir<MU, CB, true>(psiB, t, Ub + t * 9, a, on && xm == 0, g, acc);
   }
 }
 
@@ -224,10 +255,12 @@ WL_D bool row_wait(const RowHopArgs& A, unsigned long long* bar, unsigned parity
 }
 
 template <bool DAG>
-__global__ void __launch_bounds__(3 * kRowMaxLt) row_hop_kernel(RowHopArgs A) {
+__global__ void __launch_bounds__(3 * kRowMaxLt) row_hop_kernel(const __grid_constant__ CUtensorMap psimap,
+                                                                 RowHopArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);
-  unsigned char* bufs = smem + 128;
+  // stage buffers start at the first 1024-byte boundary past the barriers (swizzle atom)
+  unsigned char* bufs = smem + 128u + ((1024u - ((smem_u32(smem) + 128u) & 1023u)) & 1023u);
   const Geom& g = A.g;
   const int Lt = g.L[3];
   const int nrows = g.V / Lt;
@@ -246,7 +279,7 @@ __global__ void __launch_bounds__(3 * kRowMaxLt) row_hop_kernel(RowHopArgs A) {
   }
   __syncthreads();
   if (tid == 0)
-    for (int k = 0; k < kRowBufs && k < nst; ++k) row_stage_issue(A, row_stage_of(k), bufs + k * sbytes, &bars[k]);
+    for (int k = 0; k < kRowBufs && k < nst; ++k) row_stage_issue(A, &psimap, row_stage_of(k), bufs + k * sbytes, &bars[k]);
   cplx<double> acc[4];
   for (int k = 0; k < nst; ++k) {
     const RowStage s = row_stage_of(k);
@@ -296,7 +329,7 @@ __global__ void __launch_bounds__(3 * kRowMaxLt) row_hop_kernel(RowHopArgs A) {
     // the buffer is free once every thread has read it; then refill it
     fence_proxy_async_smem();
     __syncthreads();
-    if (tid == 0 && k + kRowBufs < nst) row_stage_issue(A, row_stage_of(k + kRowBufs), bufs + slot * sbytes, &bars[slot]);
+    if (tid == 0 && k + kRowBufs < nst) row_stage_issue(A, &psimap, row_stage_of(k + kRowBufs), bufs + slot * sbytes, &bars[slot]);
   }
 }
 
