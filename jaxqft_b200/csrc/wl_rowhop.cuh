@@ -82,6 +82,13 @@ WL_D const double2* swz_psi(const unsigned char* chunk, int site, int comp) {
 // order this thread's earlier generic-proxy shared-memory accesses before later async-proxy ones
 WL_D void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// Links staged in shared memory (1) or read through L1 from global memory (0):
+// without them a stage is 384*Lt bytes instead of 672*Lt and twice as many
+// blocks fit on an SM, but the link loads then stall the stencil (measured at
+// 24^3x48: 0.33 ms against 0.25 ms with staged links).
+#ifndef WL_ROW_LINKS_SMEM
+#define WL_ROW_LINKS_SMEM 1
+#endif
 #ifndef WL_ROW_BUFS
 #define WL_ROW_BUFS 2
 #endif
@@ -110,7 +117,9 @@ struct RowStage {
 
 // psi chunks padded to 1024 bytes (swizzle atom), link chunks after them
 WL_HD size_t row_psi_pad(int Lt) { return (((size_t)192 * Lt + 1023) / 1024) * 1024; }
-WL_HD size_t row_stage_bytes(int Lt) { return ((2 * row_psi_pad(Lt) + (size_t)288 * Lt + 1023) / 1024) * 1024; }
+WL_HD size_t row_stage_bytes(int Lt) {
+  return ((2 * row_psi_pad(Lt) + (WL_ROW_LINKS_SMEM ? (size_t)288 * Lt : 0) + 1023) / 1024) * 1024;
+}
 
 WL_D RowStage row_stage_of(int k) {
   RowStage s;
@@ -132,10 +141,11 @@ WL_D void row_stage_issue(const RowHopArgs& A, const CUtensorMap* psimap, const 
   const unsigned sp = 192u * (unsigned)Lt;
   const int line0 = (int)(((long long)rhs * g.V) * 3 / 2);  // first 128-byte line of this RHS
   const int lpr = Lt * 3 / 2;                               // lines per row (Lt even)
+  const unsigned lkb = WL_ROW_LINKS_SMEM ? (unsigned)lk : 0u;
   if (st.mu == 3) {
-    mbar_expect_tx(bar, (unsigned)(sp + lk));
+    mbar_expect_tx(bar, sp + lkb);
     tma_g2s_2d(buf, psimap, 0, line0 + row * lpr, bar);
-    bulk_g2s(buf + 2 * spad, A.U + ((size_t)3 * g.V + (size_t)row * Lt) * 9, (unsigned)lk, bar);
+    if (WL_ROW_LINKS_SMEM) bulk_g2s(buf + 2 * spad, A.U + ((size_t)3 * g.V + (size_t)row * Lt) * 9, (unsigned)lk, bar);
     return;
   }
   // row = (x*Ly + y)*Lz + z ; neighbour rows along mu with periodic wrap
@@ -144,11 +154,13 @@ WL_D void row_stage_issue(const RowHopArgs& A, const CUtensorMap* psimap, const 
   const int xm = (row / stride) % Lm;
   const int rp = row + (xm == Lm - 1 ? -(Lm - 1) * stride : stride);
   const int rm = row + (xm == 0 ? (Lm - 1) * stride : -stride);
-  mbar_expect_tx(bar, (unsigned)(2 * sp + 2 * lk));
+  mbar_expect_tx(bar, 2 * sp + 2 * lkb);
   tma_g2s_2d(buf, psimap, 0, line0 + rp * lpr, bar);
   tma_g2s_2d(buf + spad, psimap, 0, line0 + rm * lpr, bar);
-  bulk_g2s(buf + 2 * spad, A.U + ((size_t)st.mu * g.V + (size_t)row * Lt) * 9, (unsigned)lk, bar);
-  bulk_g2s(buf + 2 * spad + lk, A.U + ((size_t)st.mu * g.V + (size_t)rm * Lt) * 9, (unsigned)lk, bar);
+  if (WL_ROW_LINKS_SMEM) {
+    bulk_g2s(buf + 2 * spad, A.U + ((size_t)st.mu * g.V + (size_t)row * Lt) * 9, (unsigned)lk, bar);
+    bulk_g2s(buf + 2 * spad + lk, A.U + ((size_t)st.mu * g.V + (size_t)rm * Lt) * 9, (unsigned)lk, bar);
+  }
 }
 
 // One direction for thread (site t, colour a): acc[s] += [(1 + C g_mu) W psi]_s,a with W = ph*U
@@ -183,7 +195,11 @@ WL_D void row_dir(const unsigned char* chunk, int site, const double2* u, int a,
   cplx<double> uh[2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
   for (int b = 0; b < 3; ++b) {
+#if WL_ROW_LINKS_SMEM
     const double2 w = DAGU ? u[b * 3 + a] : u[a * 3 + b];
+#else
+    const double2 w = ldg(u + (DAGU ? b * 3 + a : a * 3 + b));
+#endif
     const cplx<double> wc{w.x, w.y};
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
@@ -231,8 +247,19 @@ WL_D void row_stage_compute(const RowHopArgs& A, const unsigned char* buf, int r
   const size_t spad = row_psi_pad(Lt), lk = (size_t)144 * Lt;
   const unsigned char* psiA = buf;
   const unsigned char* psiB = buf + spad;
+#if WL_ROW_LINKS_SMEM
   const double2* Uf = reinterpret_cast<const double2*>(buf + 2 * spad);
   const double2* Ub = reinterpret_cast<const double2*>(buf + 2 * spad + lk);
+#else
+  (void)lk;
+  const double2* Uf = A.U + ((size_t)MU * g.V + (size_t)row * Lt) * 9;  // own row of U_mu
+  const double2* Ub = Uf;
+  if (MU < 3) {  // row x - mu of U_mu
+    const int stride = g.strideRow[MU], Lm = g.L[MU];
+    const int xm_ = (row / stride) % Lm;
+    Ub = A.U + ((size_t)MU * g.V + (size_t)(row + (xm_ == 0 ? (Lm - 1) * stride : -stride)) * Lt) * 9;
+  }
+#endif
   if (MU == 3) {
     const int tp = t == Lt - 1 ? 0 : t + 1, tm = t == 0 ? Lt - 1 : t - 1;
     const bool on = g.ph_on[3] != 0;
