@@ -281,23 +281,80 @@ WL_D void color_mul_smem(const LinkSmem& L, const float2 (&h)[6], float2 (&uh)[6
   }
 }
 
+// FP16 projection: the rank-2 projection is formed on the stored half2 values
+// (packed FP16 add/FMA, one rounding to FP16) and only the six projected
+// components are converted to FP32, instead of all twelve.  For mu = 3 the
+// projection is a selection and the unused third of the spinor is not loaded.
+// Measured at 24^3x48, 16 RHS: hop 0.329 -> 0.320 ms at a lower clock, CG
+// iteration and reliable-update counts unchanged (156-165, 16).
+#ifndef WL_HALF_PROJECT
+#define WL_HALF_PROJECT 1
+#endif
+
+WL_D __half2 as_h2(unsigned int u) { return *reinterpret_cast<__half2*>(&u); }
+
+template <int MU, int C>
+WL_D float load_project_half(const SpinorField<P_HALF>& f, int rhs, unsigned c, float2 (&h)[6]) {
+  const float n = ldg(f.norm + f.nat(rhs, c));
+  __half2 s[12];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (MU == 3 && ((C > 0 && k == 2) || (C < 0 && k == 0))) continue;
+    const uint4 v = ldg(f.ptr + f.at(rhs, k, c));
+    s[4 * k + 0] = as_h2(v.x);
+    s[4 * k + 1] = as_h2(v.y);
+    s[4 * k + 2] = as_h2(v.z);
+    s[4 * k + 3] = as_h2(v.w);
+  }
+  const __half2 pcm = __floats2half2_rn((float)C, -(float)C);  // -iC x = pcm * swap(x)
+  const __half2 pmc = __floats2half2_rn(-(float)C, (float)C);  //  iC x = pmc * swap(x)
+#pragma unroll
+  for (int col = 0; col < 3; ++col) {
+    const __half2 s0 = s[col], s1 = s[3 + col], s2 = s[6 + col], s3 = s[9 + col];
+    __half2 h0, h1;
+    if (MU == 0) {
+      h0 = C > 0 ? __hadd2(s0, s3) : __hsub2(s0, s3);
+      h1 = C > 0 ? __hadd2(s1, s2) : __hsub2(s1, s2);
+    } else if (MU == 1) {
+      h0 = __hfma2(pcm, __lowhigh2highlow(s3), s0);  // s0 - iC s3
+      h1 = __hfma2(pmc, __lowhigh2highlow(s2), s1);  // s1 + iC s2
+    } else if (MU == 2) {
+      h0 = __hfma2(pcm, __lowhigh2highlow(s2), s0);  // s0 - iC s2
+      h1 = __hfma2(pcm, __lowhigh2highlow(s3), s1);  // s1 - iC s3
+    } else {
+      h0 = C > 0 ? s0 : s2;
+      h1 = C > 0 ? s1 : s3;
+    }
+    h[col] = __half22float2(h0);
+    h[3 + col] = __half22float2(h1);
+  }
+  return n;
+}
+
 template <int MU, bool DAG, class SF>
 WL_D void lane_dir(const SF& src, const LinkSmem* Ls, const int* nbs, int rhs, float2 (&acc)[12]) {
   constexpr int CF = DAG ? +1 : -1;
   constexpr int CB = -CF;
   constexpr float W3 = (MU == 3) ? 2.0f : 1.0f;
+  constexpr bool kHalfProject = WL_HALF_PROJECT && std::is_same<SF, SpinorField<P_HALF>>::value;
 #pragma unroll
   for (int dir = 0; dir < 2; ++dir) {
     const int q = 2 * MU + dir;
-    float2 sp[12];
-    const float n = RawLoad<SF>::load(src, rhs, (long long)nbs[q], sp) * W3;
     float2 h[6], uh[6];
+    float n;
+    if constexpr (kHalfProject) {
+      n = (dir == 0 ? load_project_half<MU, CF>(src, rhs, (unsigned)nbs[q], h)
+                    : load_project_half<MU, CB>(src, rhs, (unsigned)nbs[q], h)) * W3;
+    } else {
+      float2 sp[12];
+      n = RawLoad<SF>::load(src, rhs, (long long)nbs[q], sp) * W3;
+      if (dir == 0) project2<MU, CF>(sp, h);
+      else project2<MU, CB>(sp, h);
+    }
     if (dir == 0) {
-      project2<MU, CF>(sp, h);
       color_mul_smem<false>(Ls[q], h, uh);
       accum2<MU, CF>(acc, uh, n);
     } else {
-      project2<MU, CB>(sp, h);
       color_mul_smem<true>(Ls[q], h, uh);
       accum2<MU, CB>(acc, uh, n);
     }

@@ -279,7 +279,13 @@ def summarize(done: Sequence[Request], wall: float) -> dict:
     nsol = sum(r.nrhs for r in done)
     res = max((s["true_res"] for r in done for s in r.stats), default=0.0)
     conv = all(s["status"] == L.SLOT_CONVERGED for r in done for s in r.stats)
+    per_vol = {}
+    for vol in sorted({r.volume for r in done}, key=lambda v: int(np.prod(v))):
+        lv = np.array([r.latency_ms for r in done if r.volume == vol])
+        per_vol["x".join(map(str, vol))] = {"requests": int(lv.size), "p50_ms": float(np.percentile(lv, 50)),
+                                            "p99_ms": float(np.percentile(lv, 99))}
     return {"requests": len(done), "solves": nsol, "wall_s": wall, "solves_per_s": nsol / wall if wall > 0 else 0.0,
             "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
             "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
-            "mean_ms": float(lat.mean()) if len(lat) else None, "max_true_res": res, "all_converged": conv}
+            "mean_ms": float(lat.mean()) if len(lat) else None, "max_true_res": res, "all_converged": conv,
+            "per_volume": per_vol}
