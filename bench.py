@@ -271,28 +271,60 @@ def run_ours(args):
     dslash["frac"] = dslash["achieved"] / peaks()[0]
     del psi1, dout
 
-    # ---- e2e through the public API from pinned host buffers
+    # ---- e2e through the public API from pinned host buffers: a stream of K
+    # steps, each = host->device copy of its 16 RHS, ctx.solve, device->host copy
+    # of its 16 solutions; the copies of neighbouring steps run on a copy stream
+    # while the solver runs (double-buffered), and the timed region (CUDA events
+    # on the compute stream, after the copy stream drained) spans all K steps.
     e2e = None
     if rank == 0 or True:
-        b_host = b.cpu().pin_memory()
-        x_host = torch.empty_like(b_host).pin_memory()
+        b_host = [b.cpu().pin_memory(), b.cpu().pin_memory()]
+        x_host = [torch.empty_like(b_host[0]).pin_memory(), torch.empty_like(b_host[0]).pin_memory()]
+        b_dev = [torch.empty_like(b), torch.empty_like(b)]
         cur = torch.cuda.current_stream(dev)
+        cps = torch.cuda.Stream(dev)
 
-        def e2e_once():
-            bd = b_host.to(dev, non_blocking=True)
-            xd, st = ctx.solve(gauge, bd, MASS, op="eo_normal", tol=TOL, maxiter=4000, inner="half")
-            x_host.copy_(xd, non_blocking=True)
-            return st
+        def e2e_stream(K):
+            ev_in = [torch.cuda.Event(), torch.cuda.Event()]
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            e0.record(cur)
+            cps.wait_event(e0)
+            with torch.cuda.stream(cps):
+                b_dev[0].copy_(b_host[0], non_blocking=True)
+                ev_in[0].record(cps)
+            last = None
+            for i in range(K):
+                cur.wait_event(ev_in[i % 2])
+                if i + 1 < K:
+                    with torch.cuda.stream(cps):
+                        b_dev[(i + 1) % 2].copy_(b_host[(i + 1) % 2], non_blocking=True)
+                        ev_in[(i + 1) % 2].record(cps)
+                xd, st = ctx.solve(gauge, b_dev[i % 2], MASS, op="eo_normal", tol=TOL, maxiter=4000, inner="half")
+                done = torch.cuda.Event()
+                done.record(cur)
+                cps.wait_event(done)
+                with torch.cuda.stream(cps):
+                    x_host[i % 2].copy_(xd, non_blocking=True)
+                    xd.record_stream(cps)
+                last = st
+            drained = torch.cuda.Event()
+            drained.record(cps)
+            cur.wait_event(drained)
+            e1.record(cur)
+            e1.synchronize()
+            return e0.elapsed_time(e1) / 1e3, last
 
-        e2e_once()
-        te = []
-        for _ in range(max(1, min(args.steps, 3))):
-            t, st = timed(e2e_once, cur)
-            te.append(t)
-        _, e2e_value = aggregate_over_ranks(float(np.mean(te)), NRHS, dist, dev)
-        nbytes = b_host.numel() * b_host.element_size()
+        e2e_stream(2)  # warm-up
+        K = max(3, min(args.steps, 5))
+        t_all, st = e2e_stream(K)
+        _, e2e_value = aggregate_over_ranks(t_all / K, NRHS, dist, dev)
+        nbytes = b_host[0].numel() * b_host[0].element_size()
         e2e = {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(nbytes),
-               "d2h_bytes_per_step": int(nbytes)}
+               "d2h_bytes_per_step": int(nbytes), "steps": K,
+               "note": "copies of neighbouring steps overlap the solve (copy stream, double buffers)",
+               "all_converged": all(s["status"] == 2 for s in st)}
+        del b_dev, b_host, x_host
 
     # ---- serving: Poisson stream of propagator requests, continuous batching
     serve = None

@@ -1889,11 +1889,14 @@ extern "C" wl_status wl_solve(wl_ctx* ctx, wl_gauge* G, const wl_solve_params* p
   }
   if (E) {
     E->gauge = G;  // wl_engine_step rebuilds the graph when the gauge id changed
+    const bool delta_changed = E->prm.delta != prm->delta;
     E->prm = *prm;
     if (E->prm.maxiter <= 0) E->prm.maxiter = 1000;
     if (E->prm.check_every <= 0) E->prm.check_every = 8;
     E->h_maxiter.assign(E->n, E->prm.maxiter);
-    if (E->gexec) {  // delta is captured by value in the scalar kernels
+    // delta is the only solve parameter captured by value in the graph (per-RHS
+    // masses, tolerances and iteration limits live in device arrays)
+    if (E->gexec && delta_changed) {
       cudaGraphExecDestroy(E->gexec);
       E->gexec = nullptr;
       E->graph_built = false;
