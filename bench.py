@@ -462,7 +462,7 @@ def run_reference(args):
     per = float(np.mean(per_step))
     iters = args.ref_iters
     value = 1.0 / (per * iters)
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 0,
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * its * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, SHAPE)), "kappa": KAPPA},
