@@ -206,11 +206,13 @@ class WilsonNf2PseudofermionMonomial(_PFBase):
     def action(self, q):
         if self.phi is None:
             self.refresh(q, traj_length=1.0)
-        x = self.model.solve_normal(q, self.phi, tol=self.model.action_cg_tol)
-        return torch.stack([_vdot(self.phi[b], x[b]).real for b in range(x.shape[0])])
+        return self.model.pseudofermion_action(q, self.phi, tol=self.model.action_cg_tol)
 
     def force_analytic(self, q, phi):
         m = self.model
+        if m.solver_form != "normal":  # D^dag Y = phi, D X = Y (:360-362)
+            x, y = m.solve_split_with_intermediate(q, phi)
+            return m.pseudofermion_force_from_solution(q, x, y)
         x0 = self._guess()
         x = m.solve_normal(q, phi) if x0 is None else m.solve_normal_with_guess(q, phi, x0)
         y = m.apply_D(q, x)
@@ -245,11 +247,13 @@ class WilsonNf2EOPreconditionedMonomial(_PFBase):
     def action(self, q):
         if self.phi is None:
             self.refresh(q, traj_length=1.0)
-        x = self.model.solve_eop_even_normal(q, self.phi, tol=self.model.action_cg_tol)
-        return torch.stack([_vdot(self.phi[b], x[b]).real for b in range(x.shape[0])])
+        return self.model.eop_pseudofermion_action(q, self.phi, tol=self.model.action_cg_tol)
 
     def force_analytic(self, q, phi):
         m = self.model
+        if m.solver_form != "normal":  # M^dag Y_e = phi_e, M X_e = Y_e (:563-564)
+            xe, ye = m.solve_eop_even_split_with_intermediate(q, phi)
+            return m.eop_pseudofermion_force_from_solution(q, xe, ye)
         x0 = self._guess()
         xe = m.solve_eop_even_normal(q, phi) if x0 is None else m.solve_eop_even_normal_with_guess(q, phi, x0)
         ye = m.apply_eo_schur_even(q, xe, normalized=True)
@@ -310,8 +314,6 @@ class SU3WilsonNf2(SU3YangMills):
             raise ValueError("solver_form must be one of: normal, split, eo_split")
         if self.solver_form in ("split", "eo_split") and self.solver_kind == "cg":
             raise ValueError("solver_form=split/eo_split requires a non-Hermitian solver (use solver_kind=bicgstab)")
-        if self.solver_kind != "cg" or self.solver_form != "normal":
-            raise NotImplementedError("the B200 path implements the CG / normal-equation solver forms")
         if self.preconditioner_kind not in ("none", "jacobi"):
             raise ValueError("preconditioner_kind must be one of: none, jacobi")
         if self.solver_guess_mode not in ("last", "poly", "mre"):
@@ -405,13 +407,16 @@ class SU3WilsonNf2(SU3YangMills):
     def _out(self, x: torch.Tensor) -> torch.Tensor:
         return x if self.dtype == torch.complex128 else x.to(self.dtype)
 
-    def _apply(self, op: str, U, psi, normalized: bool = False):
+    def _apply_raw(self, op: str, U, psi, normalized: bool = False) -> torch.Tensor:
         gauges = self._gauges_for(U)
         psi = self._as_tensor(psi)
         out = torch.empty_like(psi)
         for b in range(psi.shape[0]):
             self.ctx.apply(op, gauges[b], self.mass, psi[b], normalized=normalized, out=out[b])
-        return self._out(out)
+        return out
+
+    def _apply(self, op: str, U, psi, normalized: bool = False):
+        return self._out(self._apply_raw(op, U, psi, normalized))
 
     # ------------------------------------------------------------------ shapes / EO helpers
     def fermion_shape(self) -> Tuple[int, ...]:
@@ -503,6 +508,9 @@ class SU3WilsonNf2(SU3YangMills):
 
     # ------------------------------------------------------------------ solves (:1243-1454)
     def _solve(self, op: str, U, rhs, x0=None, tol: Optional[float] = None):
+        return self._out(self._solve_raw(op, U, rhs, x0, tol))
+
+    def _solve_raw(self, op: str, U, rhs, x0=None, tol: Optional[float] = None) -> torch.Tensor:
         gauges = self._gauges_for(U)
         tol = self.cg_tol if tol is None else float(tol)
         rhs = self._as_tensor(rhs)
@@ -520,7 +528,7 @@ class SU3WilsonNf2(SU3YangMills):
             raise L.WilsonError(L.WL_ERR_NAN, "solver produced a non-finite residual")
         if any(s["status"] != L.SLOT_CONVERGED for s in stats):
             warnings.warn(f"CG did not reach tol {tol} within {self.cg_maxiter} iterations", RuntimeWarning)
-        return self._out(out)
+        return out
 
     def solve_normal(self, U, phi, tol: Optional[float] = None):
         return self._solve("normal", U, phi, tol=tol)
@@ -534,11 +542,89 @@ class SU3WilsonNf2(SU3YangMills):
     def solve_eop_even_normal_with_guess(self, U, rhs, x0):
         return self._solve("eo_normal", U, self._project_even(rhs), self._project_even(x0))
 
+    # Non-Hermitian solves (:1271-1454).  The reference runs BiCGStab / GMRES on D (or on the
+    # Schur operator); here every one of them is the batched mixed-precision CG on the normal
+    # equations of the same operator (CGNR): A x = b  <=>  A^dag A x = A^dag b, and
+    # A^dag y = b  <=>  y = A (A^dag A)^-1 b.  The solution is the same to solver tolerance;
+    # ``cg_tol`` bounds the normal-equation residual.  ``solver_kind`` bicgstab / gmres and
+    # ``gmres_restart`` are accepted for configuration compatibility and select the same CGNR.
+    def solve_direct(self, U, rhs, tol: Optional[float] = None):
+        """x = D^-1 rhs (:1271-1284)."""
+        return self._out(self._solve_raw("normal", U, self._apply_raw("DDAG", U, rhs), tol=tol))
+
+    def solve_dagger(self, U, rhs, tol: Optional[float] = None):
+        """y = D^-dag rhs (:1286-1299)."""
+        return self._out(self._apply_raw("D", U, self._solve_raw("normal", U, rhs, tol=tol)))
+
+    def _solve_eo(self, U, rhs, which: str, tol: Optional[float] = None) -> torch.Tensor:
+        """D x = b (which="direct") or D^dag x = b ("dagger") through the even Schur complement
+        and odd-site reconstruction (:1301-1336).  With K = A - m0 (A = D or D^dag):
+        rhs_e = b_e - P_e K b_o / m0, S x_e = rhs_e with S = m0 M for "direct" and m0 M^dag for
+        "dagger" (M the normalized even Schur operator), x_o = (b_o - P_o K x_e) / m0."""
+        if which not in ("direct", "dagger"):
+            raise ValueError(f"Unknown EO solve kind: {which}")
+        op = "D" if which == "direct" else "DDAG"
+        m0 = self._m0
+        b = self._as_tensor(rhs)
+        b_e, b_o = self._project_even(b), self._project_odd(b)
+        rhs_e = b_e - self._project_even(self._apply_raw(op, U, b_o) - m0 * b_o) / m0
+        if which == "direct":  # M x_e = rhs_e / m0  <=>  M^dag M x_e = M^dag rhs_e / m0
+            rhs_n = self._apply_raw("SCHUR_E_DAG", U, rhs_e / m0, normalized=True)
+            x_e = self._project_even(self._solve_raw("eo_normal", U, rhs_n, tol=tol))
+        else:  # M^dag x_e = rhs_e / m0  <=>  x_e = M (M^dag M)^-1 rhs_e / m0
+            z_e = self._project_even(self._solve_raw("eo_normal", U, rhs_e / m0, tol=tol))
+            x_e = self._project_even(self._apply_raw("SCHUR_E", U, z_e, normalized=True))
+        x_o = (b_o - self._project_odd(self._apply_raw(op, U, x_e) - m0 * x_e)) / m0
+        return x_e + x_o
+
+    def solve_direct_eo(self, U, rhs, tol: Optional[float] = None):
+        return self._out(self._solve_eo(U, rhs, "direct", tol))
+
+    def solve_dagger_eo(self, U, rhs, tol: Optional[float] = None):
+        return self._out(self._solve_eo(U, rhs, "dagger", tol))
+
+    def solve_eop_even_direct(self, U, rhs, tol: Optional[float] = None):
+        """M x_e = rhs_e, M the normalized even Schur operator (:1338-1350)."""
+        rhs_n = self._apply_raw("SCHUR_E_DAG", U, self._project_even(rhs), normalized=True)
+        return self._out(self._project_even(self._solve_raw("eo_normal", U, rhs_n, tol=tol)))
+
+    def solve_eop_even_dagger(self, U, rhs, tol: Optional[float] = None):
+        """M^dag y_e = rhs_e (:1352-1364)."""
+        z = self._project_even(self._solve_raw("eo_normal", U, self._project_even(rhs), tol=tol))
+        return self._out(self._project_even(self._apply_raw("SCHUR_E", U, z, normalized=True)))
+
+    def solve_eop_even_split_with_intermediate(self, U, phi, tol: Optional[float] = None):
+        """y = M^-dag phi, x = M^-1 y (:1394-1397).  With y = M z, z = (M^dag M)^-1 phi, the second
+        system M^dag M x = M^dag y has the solution x = z, so the pair costs one solve."""
+        z = self._project_even(self._solve_raw("eo_normal", U, self._project_even(phi), tol=tol))
+        y = self._project_even(self._apply_raw("SCHUR_E", U, z, normalized=True))
+        return self._out(z), self._out(y)
+
+    def solve_eop_even_split(self, U, phi):
+        return self.solve_eop_even_split_with_intermediate(U, phi)[0]
+
+    def solve_split_with_intermediate(self, U, phi, tol: Optional[float] = None):
+        """y = D^-dag phi, x = D^-1 y (:1438-1445).  "split": y = D z with z = (D^dag D)^-1 phi and
+        x = z (the second normal system D^dag D x = D^dag y has the solution z), one solve;
+        "eo_split": both solves through the even Schur complement."""
+        if self.solver_form == "eo_split":
+            y = self._solve_eo(U, phi, "dagger", tol)
+            return self._out(self._solve_eo(U, y, "direct", tol)), self._out(y)
+        z = self._solve_raw("normal", U, phi, tol=tol)
+        return self._out(z), self._out(self._apply_raw("D", U, z))
+
+    def solve_split(self, U, phi):
+        return self.solve_split_with_intermediate(U, phi)[0]
+
     def solve_pseudofermion(self, U, phi):
-        return self.solve_normal(U, phi)
+        if self.solver_form == "normal":
+            return self.solve_normal(U, phi)
+        return self.solve_split(U, phi)
 
     def solve_eop_even(self, U, phi):
-        return self.solve_eop_even_normal(U, phi)
+        if self.solver_form == "normal":
+            return self.solve_eop_even_normal(U, phi)
+        return self.solve_eop_even_split(U, phi)
 
     def normal_residual_stats(self, U, phi, x) -> Dict[str, float]:
         r = self.apply_normal(U, x) - self._as_tensor(phi)
@@ -558,15 +644,30 @@ class SU3WilsonNf2(SU3YangMills):
                 "mean_solver_iters_stage2": float("nan")}
 
     # ------------------------------------------------------------------ actions (:1183-1208)
-    def pseudofermion_action(self, U, phi):
-        phi = self._as_tensor(phi)
-        x = self.solve_normal(U, phi).to(torch.complex128)
-        return torch.stack([_vdot(phi[b], x[b]).real for b in range(phi.shape[0])])
+    def _split_chi(self, U, phi, eo_prec: bool, tol: Optional[float] = None) -> torch.Tensor:
+        """chi with A^dag chi = phi: S_pf = phi^dag (A^dag A)^-1 phi = chi^dag chi (:1190-1197)."""
+        if eo_prec:
+            z = self._project_even(self._solve_raw("eo_normal", U, self._project_even(phi), tol=tol))
+            return self._project_even(self._apply_raw("SCHUR_E", U, z, normalized=True))
+        if self.solver_form == "eo_split":
+            return self._solve_eo(U, phi, "dagger", tol)
+        return self._apply_raw("D", U, self._solve_raw("normal", U, phi, tol=tol))
 
-    def eop_pseudofermion_action(self, U, phi):
+    def pseudofermion_action(self, U, phi, tol: Optional[float] = None):
+        phi = self._as_tensor(phi)
+        if self.solver_form == "normal":
+            x = self._solve_raw("normal", U, phi, tol=tol)
+            return torch.stack([_vdot(phi[b], x[b]).real for b in range(phi.shape[0])])
+        chi = self._split_chi(U, phi, False, tol)
+        return torch.stack([_vdot(chi[b], chi[b]).real for b in range(chi.shape[0])])
+
+    def eop_pseudofermion_action(self, U, phi, tol: Optional[float] = None):
         phi = self._project_even(phi)
-        x = self.solve_eop_even_normal(U, phi).to(torch.complex128)
-        return torch.stack([_vdot(phi[b], x[b]).real for b in range(phi.shape[0])])
+        if self.solver_form == "normal":
+            x = self._solve_raw("eo_normal", U, phi, tol=tol)
+            return torch.stack([_vdot(phi[b], x[b]).real for b in range(phi.shape[0])])
+        chi = self._split_chi(U, phi, True, tol)
+        return torch.stack([_vdot(chi[b], chi[b]).real for b in range(chi.shape[0])])
 
     # ------------------------------------------------------------------ forces (:1556-1597)
     def pseudofermion_force_from_solution(self, U, X, Y):
