@@ -15,8 +15,10 @@ Reported: value = solves/s of that batched mixed solve (device time, CUDA
 events on the solver stream, inputs resident in HBM), next to plain FP64 CG
 (one RHS at a time) on the same systems; e2e = the same solve through the
 public API from pinned host buffers with host<->device copies timed; the
-roofline of the dominant kernel (the FP16 16-RHS hop) measured live; and a
-CPU baseline (the C restatement of the reference's CG on the host cores).
+roofline of the dominant kernel (the FP16 16-RHS hop) measured live; the
+Dslash bandwidth (FP64, 1 RHS) in the internal layout and in the reference
+layout; and a CPU baseline (the C restatement of the reference's CG on the
+host cores).
 
 Data is synthetic (seeded); every working set is larger than the 126 MB L2.
 
@@ -242,6 +244,15 @@ def run_ours(args):
         t64 += t
         it64.append(st[0]["iters"])
     fp64_sps = n64 / t64
+    # the Dslash in the internal layout (the EO hop K_oe of that FP64 CG: SoA FP64 spinors, 18-real FP64
+    # links, 1 RHS; 8 links + 2 spinors per target site), timed alone with CUDA events on the engine stream
+    eng64.time_hop(reps=5)
+    n_ms, n_bytes = eng64.time_hop(reps=50)
+    dslash_native = {"kernel": "EO hop K_oe, internal SoA layout, FP64 (18-real links), 1 RHS (autotuned shape)",
+                     "ms_per_launch": n_ms, "algorithmic_bytes_per_launch": n_bytes,
+                     "achieved": n_bytes / (n_ms * 1e-3) / 1e9, "unit": "GB/s"}
+    dslash_native["frac"] = dslash_native["achieved"] / peaks()[0]
+    dslash_native["peak"] = peaks()[0]
     eng64.close()
 
     # ---- live roofline of the dominant kernel (FP16 hop over 16 RHS)
@@ -364,7 +375,8 @@ def run_ours(args):
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": hop_bytes,
                          "ms_per_launch": hop_ms, "traffic": traffic},
-            "dslash_fp64": dslash,
+            "dslash": dslash_native,
+            "dslash_fp64_reference_layout": dslash,
             "e2e": e2e,
             "serve": serve,
             "gpu_launches": int(launches),
@@ -475,9 +487,10 @@ def run_reference(args):
 
 
 def run_profile_dslash(args):
-    """Profiling driver for the drop-in FP64 Dslash (reference layout, 1 RHS):
-    3 warm-up applications, then `--profile-dslash` applications of D between
-    cudaProfilerStart/Stop."""
+    """Profiling driver for the FP64 Dslash, 1 RHS: the drop-in D on the reference
+    layout (3 warm-up applications, then `--profile-dslash` applications between
+    cudaProfilerStart/Stop), or with --dslash-layout internal the EO hop of the
+    FP64 engine (one more launch inside the range)."""
     import torch
 
     from jaxqft_b200 import lib as L
@@ -488,6 +501,18 @@ def run_profile_dslash(args):
     ctx = L.WilsonContext(SHAPE, bc=BC, device=dev)
     U, eta = make_inputs(torch, dev, seed=0)
     gauge = ctx.gauge(U)
+    if args.dslash_layout == "internal":  # the EO hop of the FP64 1-RHS engine (SoA fields, 18-real links)
+        del U, eta
+        eng = L.Engine(ctx, gauge, 1, op="eo_normal", inner="double", tol=TOL, maxiter=10)
+        eng.time_hop(reps=3)
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()
+        ms, byts = eng.time_hop(reps=args.profile_dslash)
+        torch.cuda.cudart().cudaProfilerStop()
+        eng.close()
+        print(json.dumps({"profile": "FP64 EO hop, internal layout, 1 RHS", "shape": SHAPE, "ms": ms,
+                          "GBps": byts / ms / 1e6}), flush=True)
+        return
     psi = eta[NRHS - 1:NRHS].contiguous()
     del U, eta
     out = torch.empty_like(psi)
@@ -568,7 +593,9 @@ def main():
                     help="FP64 CG iterations to 1e-10 on this system: plain FP64 CG needs 152-154 on each of the "
                          "16 RHS (measured with --fp64-all)")
     ap.add_argument("--profile-dslash", type=int, default=0,
-                    help="profiling driver: this many FP64 reference-layout D applications (on --shape)")
+                    help="profiling driver: this many FP64 Dslash applications (on --shape)")
+    ap.add_argument("--dslash-layout", default="reference", choices=["reference", "internal"],
+                    help="--profile-dslash: reference-layout D, or the internal-layout EO hop")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -177,6 +177,7 @@ static SpinorRef sref(const void* p, const Geom& g) {
 struct Tune {
   int nr = 1, bx = 128, by = 1;
   int lanes = 0;  // > 0: RHS-in-lanes hop (FP16/FP32 storage) with this many RHS lanes per site
+  int pair = 0;   // 1: FP64 single-RHS stencil with two threads per site (hop_pair_kernel)
 };
 
 static dim3 grid_for(const Geom& g, const Tune& t, int nrhs, int npar) {
@@ -184,6 +185,7 @@ static dim3 grid_for(const Geom& g, const Tune& t, int nrhs, int npar) {
     const int S = kLaneBlock / t.lanes;
     return dim3((g.Vh + S - 1) / S, (nrhs + t.lanes - 1) / t.lanes, npar);
   }
+  if (t.pair) return dim3((g.Vh + t.bx / 2 - 1) / (t.bx / 2), nrhs, npar);
   int groups = (nrhs + t.nr - 1) / t.nr;
   return dim3((g.Vh + t.bx - 1) / t.bx, (groups + t.by - 1) / t.by, npar);
 }
@@ -233,6 +235,10 @@ static void launch_hop_impl(const Tune& t, const HopArgs<LF, SF, EPI>& a, int np
         case 8: hop_lanes_d_kernel<DAG, 8><<<grid, lb, 0, st>>>(a); break;
         default: hop_lanes_d_kernel<DAG, 4><<<grid, lb, 0, st>>>(a); break;
       }
+      return;
+    }
+    if (t.pair) {
+      hop_pair_kernel<DAG><<<grid, dim3(t.bx, 1, 1), 0, st>>>(a);
       return;
     }
   }
@@ -1372,6 +1378,13 @@ static Tune autotune_hop(wl_engine* E, cudaStream_t st) {
         cands.push_back(Tune{nr, bx, by});
       }
   }
+  if (S == P_DOUBLE && !E->lanes_mode)
+    for (int bx : {64, 128, 256}) {
+      Tune t;
+      t.bx = bx;
+      t.pair = 1;
+      cands.push_back(t);
+    }
   if (E->lanes_mode) {
     for (int lanes : {4, 8, 16}) {
       if (lanes > n && lanes > 4) continue;
@@ -1397,17 +1410,19 @@ static Tune autotune_hop(wl_engine* E, cudaStream_t st) {
   A.epi.has_self = 0;
   A.epi.b = E->neg_half;
   const int reps = g.Vh >= 65536 ? 5 : 20;
-  for (const Tune& t : cands) {
+  for (const Tune& t : cands) {  // best of three timings per candidate (shapes within a few % of each other)
     launch_hop<false, IdxCompact>(t, A, 1, st);
-    cudaEventRecord(e0, st);
-    for (int i = 0; i < reps; ++i) launch_hop<false, IdxCompact>(t, A, 1, st);
-    cudaEventRecord(e1, st);
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (cudaGetLastError() == cudaSuccess && ms < best_ms) {
-      best_ms = ms;
-      best = t;
+    for (int trial = 0; trial < 3; ++trial) {
+      cudaEventRecord(e0, st);
+      for (int i = 0; i < reps; ++i) launch_hop<false, IdxCompact>(t, A, 1, st);
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (cudaGetLastError() == cudaSuccess && ms < best_ms) {
+        best_ms = ms;
+        best = t;
+      }
     }
   }
   cudaEventDestroy(e0);
@@ -1416,16 +1431,20 @@ static Tune autotune_hop(wl_engine* E, cudaStream_t st) {
 }
 
 static Tune pick_tune(wl_engine* E, cudaStream_t st) {
-  // WL_FORCE_TUNE="nr,bx,by,lanes" pins the hop shape (tests exercise every shape this way)
+  // WL_FORCE_TUNE="nr,bx,by,lanes[,pair]" pins the hop shape (tests exercise every shape this way)
   if (const char* f = std::getenv("WL_FORCE_TUNE")) {
     Tune t;
-    if (std::sscanf(f, "%d,%d,%d,%d", &t.nr, &t.bx, &t.by, &t.lanes) == 4) {
+    const int nf = std::sscanf(f, "%d,%d,%d,%d,%d", &t.nr, &t.bx, &t.by, &t.lanes, &t.pair);
+    if (nf == 4) t.pair = 0;
+    if (nf >= 4) {
       const bool lanes_ok = t.lanes == 0 || t.lanes == 4 || t.lanes == 8 || t.lanes == 16;
       const bool nr_ok = t.nr == 1 || t.nr == 2 || t.nr == 4;
       const bool shape_ok = t.bx % 32 == 0 && t.bx >= 64 && t.bx * t.by <= 256 && t.by * t.nr <= kMaxRB;
       if (lanes_ok && nr_ok && (t.lanes > 0 || shape_ok)) {
         if (t.lanes > 0 && !E->lanes_mode) t = Tune{};  // FP64 iteration or < 4 slots: thread-per-site kernel
         if (t.lanes > 0) t.bx = kLaneBlock;
+        if (t.pair && (E->sprec != P_DOUBLE || E->lanes_mode || t.lanes > 0)) t.pair = 0;  // FP64 sites only
+        if (t.pair) t.nr = 1, t.by = 1;
         return t;
       }
     }
@@ -1452,8 +1471,8 @@ static Tune pick_tune(wl_engine* E, cudaStream_t st) {
   }
   const char* verb = std::getenv("WL_VERBOSE");
   if (verb && verb[0] == '1')
-    std::fprintf(stderr, "[wl] tune vh=%d prec=%d nslots=%d op=%d -> nr=%d bx=%d by=%d lanes=%d\n", k.vh, k.prec,
-                 k.nslots, k.op, t.nr, t.bx, t.by, t.lanes);
+    std::fprintf(stderr, "[wl] tune vh=%d prec=%d nslots=%d op=%d -> nr=%d bx=%d by=%d lanes=%d pair=%d\n", k.vh,
+                 k.prec, k.nslots, k.op, t.nr, t.bx, t.by, t.lanes, t.pair);
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune_cache[k] = t;
   return t;

@@ -285,6 +285,148 @@ __global__ void __launch_bounds__(256) hop_kernel(HopArgs<LF, SF, EPI> A) {
   if (EPI::kReduce) reduce_rhs<NR>(red, A.red, A.nrhs, A.mask);
 }
 
+// ------------------------------------------------------------------ FP64, two threads per site
+// Single-RHS FP64 stencil with a pair of threads per target site.  Thread j
+// (j = lane & 1) forms half-spinor row j of every hop,
+//   mu=0: h = s_j + c s_{3-j}      mu=1: h = s_j + (1-2j) c' s_{3-j}
+//   mu=2: h = s_j + c' s_{2+j}     mu=3: 2 s_j (c = +1) or 2 s_{2+j} (c = -1)
+// (c' = -i c), so it loads only the two spin components it needs; both threads
+// of a pair read the same link addresses in the same instruction (one memory
+// request).  Thread j keeps three colour vectors: its own upper spin A = a_j
+// and partial sums X of a_{3-j} and Y of a_{2+j}; one xor-shuffle exchange
+// assembles the site in thread 0, which runs the epilogue.  Per thread this
+// holds about half the registers of hop_kernel, so twice as many threads per
+// SM keep neighbour loads in flight.
+template <int MU, int C>
+WL_D void pair_project(const SpinorField<P_DOUBLE>& src, int rhs, unsigned nb, int j, double sg,
+                       cplx<double> (&h)[3]) {
+  const int s1 = (MU == 3 && C < 0) ? 2 + j : j;
+  const int s2 = MU == 2 ? 2 + j : 3 - j;
+#pragma unroll
+  for (int col = 0; col < 3; ++col) {
+    const double2 a = ldg(src.ptr + src.at(rhs, s1 * 3 + col, nb));
+    if (MU == 3) {
+      h[col] = {2.0 * a.x, 2.0 * a.y};
+      continue;
+    }
+    const double2 b = ldg(src.ptr + src.at(rhs, s2 * 3 + col, nb));
+    if (MU == 0) {
+      h[col] = C > 0 ? cplx<double>{a.x + b.x, a.y + b.y} : cplx<double>{a.x - b.x, a.y - b.y};
+    } else {
+      // w = -i C b
+      const cplx<double> w = C > 0 ? mul_mi(cplx<double>{b.x, b.y}) : mul_i(cplx<double>{b.x, b.y});
+      if (MU == 1) h[col] = {fma(sg, w.re, a.x), fma(sg, w.im, a.y)};
+      else h[col] = {a.x + w.re, a.y + w.im};
+    }
+  }
+}
+
+// Accumulate colour component a of one hop, uh, into A, X, Y (see above).
+template <int MU, int C>
+WL_D void pair_accum(int a, cplx<double> uh, double sg, cplx<double> (&A)[3], cplx<double> (&X)[3],
+                     cplx<double> (&Y)[3]) {
+  if (MU == 3) {
+    if (C > 0) A[a] = A[a] + uh;
+    else Y[a] = Y[a] + uh;
+    return;
+  }
+  A[a] = A[a] + uh;
+  if (MU == 0) {
+    X[a] = C > 0 ? X[a] + uh : X[a] - uh;
+  } else if (MU == 1) {  // X += (1-2j) (i C) uh
+    const cplx<double> w = C > 0 ? mul_i(uh) : mul_mi(uh);
+    X[a] = {fma(sg, w.re, X[a].re), fma(sg, w.im, X[a].im)};
+  } else {  // Y += (i C) uh
+    Y[a] = Y[a] + (C > 0 ? mul_i(uh) : mul_mi(uh));
+  }
+}
+
+template <int MU, int C, bool DAGU>
+WL_D void pair_hop(const Link<double>& u, const cplx<double> (&h)[3], bool ph, const Geom& g, double sg,
+                   cplx<double> (&A)[3], cplx<double> (&X)[3], cplx<double> (&Y)[3]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    cplx<double> uh = {0.0, 0.0};
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      if (DAGU) fmac_(uh, u.m[b][a], h[b]);
+      else fma_(uh, u.m[a][b], h[b]);
+    }
+    if (ph) uh = uh * cplx<double>{g.ph_re[MU], DAGU ? -g.ph_im[MU] : g.ph_im[MU]};
+    pair_accum<MU, C>(a, uh, sg, A, X, Y);
+  }
+}
+
+template <int MU, bool DAG, class LF>
+WL_D void pair_dir(const Geom& g, const LF& links, const SpinorField<P_DOUBLE>& src, int parity, const Site& s,
+                   int rhs, int j, double sg, cplx<double> (&A)[3], cplx<double> (&X)[3], cplx<double> (&Y)[3]) {
+  constexpr int CF = DAG ? +1 : -1;
+  constexpr int CB = -CF;
+  {
+    const unsigned nb = (unsigned)neighbor(g, s, MU, +1);
+    Link<double> u;
+    links.load(u, parity, MU, s.c);
+    cplx<double> h[3];
+    pair_project<MU, CF>(src, rhs, nb, j, sg, h);
+    pair_hop<MU, CF, false>(u, h, g.ph_on[MU] && (s.x[MU] == g.L[MU] - 1), g, sg, A, X, Y);
+  }
+  {
+    const unsigned nb = (unsigned)neighbor(g, s, MU, -1);
+    Link<double> u;
+    links.load(u, 1 - parity, MU, (int)nb);
+    cplx<double> h[3];
+    pair_project<MU, CB>(src, rhs, nb, j, sg, h);
+    pair_hop<MU, CB, true>(u, h, g.ph_on[MU] && (s.x[MU] == 0), g, sg, A, X, Y);
+  }
+}
+
+WL_D cplx<double> shfl_pair(cplx<double> v) {
+  return {__shfl_xor_sync(0xffffffffu, v.re, 1), __shfl_xor_sync(0xffffffffu, v.im, 1)};
+}
+
+// Resident 256-thread blocks per SM: 2 caps the pair kernel at 128 registers
+// (no spills).  Measured at 24^3x48, 1 RHS: 96 us, against 148 us at 80
+// registers (3 blocks, spills) and 103 us for hop_kernel (144 registers).
+#ifndef WL_HOP_PAIR_MINB
+#define WL_HOP_PAIR_MINB 2
+#endif
+
+template <bool DAG, class LF, class EPI>
+__global__ void __launch_bounds__(256, WL_HOP_PAIR_MINB)
+    hop_pair_kernel(HopArgs<LF, SpinorField<P_DOUBLE>, EPI> A) {
+  const int c = blockIdx.x * (blockDim.x >> 1) + (threadIdx.x >> 1);
+  const int j = threadIdx.x & 1;
+  const double sg = 1.0 - 2.0 * j;
+  const int parity = A.parity0 ^ blockIdx.z;
+  const int rhs = blockIdx.y;
+  const bool act = c < A.g.Vh && rhs < A.nrhs && (A.mask == nullptr || A.mask[rhs] != 0);
+  cplx<double> Ac[3], Xc[3], Yc[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) Ac[a] = Xc[a] = Yc[a] = {0.0, 0.0};
+  Site s{};
+  if (act) {
+    s = site_from_compact(A.g, parity, c);
+    const SpinorField<P_DOUBLE>& src = A.src[1 - parity];
+    pair_dir<0, DAG>(A.g, A.links, src, parity, s, rhs, j, sg, Ac, Xc, Yc);
+    pair_dir<1, DAG>(A.g, A.links, src, parity, s, rhs, j, sg, Ac, Xc, Yc);
+    pair_dir<2, DAG>(A.g, A.links, src, parity, s, rhs, j, sg, Ac, Xc, Yc);
+    pair_dir<3, DAG>(A.g, A.links, src, parity, s, rhs, j, sg, Ac, Xc, Yc);
+  }
+  // thread 0 of the pair: a0 = A, a1 = A', a2 = Y + X', a3 = X + Y'
+  Spinor<double> acc;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const cplx<double> Ap = shfl_pair(Ac[a]), Xp = shfl_pair(Xc[a]), Yp = shfl_pair(Yc[a]);
+    acc.v[0][a] = Ac[a];
+    acc.v[1][a] = Ap;
+    acc.v[2][a] = Yc[a] + Xp;
+    acc.v[3][a] = Xc[a] + Yp;
+  }
+  double red[1] = {0.0};
+  if (act && j == 0) red[0] = A.epi(rhs, parity, s.c, acc);
+  if (EPI::kReduce) reduce_rhs<1>(red, A.red, A.nrhs, A.mask);
+}
+
 // ------------------------------------------------------------------ epilogues
 template <typename T>
 WL_D double snorm2(const Spinor<T>& s) {

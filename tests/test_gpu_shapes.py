@@ -81,3 +81,44 @@ def test_batched_solve_per_shape(setup, forced):
         ax = W.schur_even(U, s, masses[r], bc, normalized=True, dag=True)[0]
         assert np.linalg.norm(b[r] - ax) / np.linalg.norm(b[r]) <= 1e-10, (forced, r)
     eng.close()
+
+
+# (forced shape, slots): FP64 engines with fewer than four slots run the
+# thread-per-site stencils; a fifth field 1 selects two threads per site
+FP64_CASES = [("1,64,1,0,1", 1), ("1,128,1,0,1", 3), ("1,256,1,0,1", 1), ("1,128,1,0", 1), ("1,128,1,0", 3)]
+
+
+@pytest.mark.parametrize("forced,nslots", FP64_CASES, indirect=["forced"])
+def test_fp64_stencil_shapes(setup, forced, nslots):
+    """Every FP64 iterated-stencil shape gives the FP64 operator to 1e-13 and
+    solves to the FP64 true-residual tolerance."""
+    shape, U, bc, ctx, gauge, rng = setup
+    m = -0.25
+    eng = Engine(ctx, gauge, nslots, op="eo_normal", inner="double")
+    xe = W.project(W.gaussian_spinor(rng, shape, 1), 0)
+    s = W.schur_even(U, xe, m, bc, normalized=True)
+    ref = W.schur_even(U, s, m, bc, normalized=True, dag=True)
+    out = eng.debug_apply(2, m, torch.from_numpy(xe[0])).cpu().numpy()
+    assert rel(out, ref[0]) < 1e-13, forced
+    eng.close()
+    eng = Engine(ctx, gauge, nslots, op="normal", inner="double")
+    x = W.gaussian_spinor(rng, shape, 1)
+    out = eng.debug_apply(4, m, torch.from_numpy(x[0])).cpu().numpy()
+    assert rel(out, W.apply_normal(U, x, m, bc)[0]) < 1e-13, forced
+    eng.close()
+    masses = np.linspace(-0.3, 0.1, nslots)
+    b = W.project(W.gaussian_spinor(rng, shape, nslots), 0)
+    eng = Engine(ctx, gauge, nslots, op="eo_normal", inner="double", tol=1e-10, maxiter=3000)
+    eng.admit(np.arange(nslots), torch.from_numpy(b), masses)
+    na = nslots
+    while na:
+        eng.step(8)
+        _, na = eng.poll()
+    for r in range(nslots):
+        xr, st = eng.retire(r)
+        assert st["status"] == 2, (forced, r, st)
+        xr = xr.cpu().numpy()
+        s = W.schur_even(U, xr[None], masses[r], bc, normalized=True)
+        ax = W.schur_even(U, s, masses[r], bc, normalized=True, dag=True)[0]
+        assert np.linalg.norm(b[r] - ax) / np.linalg.norm(b[r]) <= 1e-10, (forced, r)
+    eng.close()
