@@ -167,6 +167,9 @@ void* wl_engine_stream(wl_engine* eng);
    Writes the mean milliseconds per launch and the algorithmic HBM bytes one
    launch must move (every link and spinor touched once). Synchronous. */
 wl_status wl_engine_time_hop(wl_engine* eng, int reps, double* ms_per_launch, double* bytes_per_launch);
+/* The same for the FP64 hop of the reliable update (x64 -> K_oe x64 over all
+   slots, with the FP64 links and the shape the update uses). */
+wl_status wl_engine_time_update_hop(wl_engine* eng, int reps, double* ms_per_launch, double* bytes_per_launch);
 /* Apply the engine's iterated (sloppy-precision) operator to one
    reference-layout field through slot 0's buffers, for testing the FP16/FP32
    operators against FP64: stage 0 -> K_oe x_e (odd sites of out), 1 -> M x_e,

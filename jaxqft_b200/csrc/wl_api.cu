@@ -1430,6 +1430,60 @@ static Tune autotune_hop(wl_engine* E, cudaStream_t st) {
   return best;
 }
 
+static float time_update_hop(wl_engine* E, cudaStream_t st, const Tune& t, int reps);
+
+// The FP64 hop of the reliable update in lanes engines: the RHS lanes per site,
+// i.e. how many sweeps over the lattice one update hop makes (nslots / lanes),
+// is chosen by timing.  With 16 FP64 RHS a site's sources are 3 KB and the
+// x-neighbour reuse distance of one sweep (2 Ly Lz Lt/2 sites) outgrows the L2,
+// so narrower sweeps can move fewer DRAM bytes even though each re-reads the links.
+static Tune pick_update_tune(wl_engine* E, cudaStream_t st) {
+  const int n = E->n;
+  Tune t;
+  t.bx = kLaneBlock;
+  t.lanes = n > 8 ? 16 : (n > 4 ? 8 : 4);
+  // WL_FORCE_UPDATE_TUNE="lanes" pins the shape
+  if (const char* f = std::getenv("WL_FORCE_UPDATE_TUNE")) {
+    int lanes = 0;
+    if (std::sscanf(f, "%d", &lanes) == 1 && (lanes == 4 || lanes == 8 || lanes == 16)) {
+      t.lanes = lanes;
+      return t;
+    }
+  }
+  TuneKey k{E->ctx->g.Vh, 100 + (E->ru_links12 ? 1 : 0), n, E->prm.op};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(k);
+    if (it != g_tune_cache.end()) return it->second;
+  }
+  const char* env = std::getenv("WL_AUTOTUNE");
+  if (!(env && env[0] == '0')) {
+    const int reps = E->ctx->g.Vh >= 65536 ? 3 : 10;
+    float best_ms = 1e30f;
+    Tune best = t;
+    for (int lanes : {4, 8, 16}) {
+      if (lanes > n && lanes > 4) continue;
+      Tune c = t;
+      c.lanes = lanes;
+      for (int trial = 0; trial < 3; ++trial) {
+        const float ms = time_update_hop(E, st, c, reps);
+        if (cudaGetLastError() == cudaSuccess && ms < best_ms) {
+          best_ms = ms;
+          best = c;
+        }
+      }
+    }
+    t = best;
+  }
+  const char* verb = std::getenv("WL_VERBOSE");
+  if (verb && verb[0] == '1')
+    std::fprintf(stderr, "[wl] update tune vh=%d links12=%d nslots=%d op=%d -> lanes=%d\n", k.vh,
+                 (int)E->ru_links12, n, k.op, t.lanes);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[k] = t;
+  return t;
+}
+
 static Tune pick_tune(wl_engine* E, cudaStream_t st) {
   // WL_FORCE_TUNE="nr,bx,by,lanes[,pair]" pins the hop shape (tests exercise every shape this way)
   if (const char* f = std::getenv("WL_FORCE_TUNE")) {
@@ -1601,7 +1655,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   E->h_maxiter.assign(n, E->prm.maxiter);
   E->ts = pick_tune(E, st);
   E->td = Tune{1, 128, 1};
-  if (E->lanes_mode) E->td.lanes = n > 8 ? 16 : (n > 4 ? 8 : 4);
+  if (E->lanes_mode) E->td = pick_update_tune(E, st);
   E->tsite = Tune{1, 128, 1};
   e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
@@ -1790,6 +1844,54 @@ extern "C" wl_status wl_engine_time_hop(wl_engine* E, int reps, double* ms, doub
   if (s != WL_OK) return s;
   *ms = (double)t / reps;
   *bytes = (double)hop_bytes(ctx->g, E->sprec, E->n);
+  return WL_OK;
+}
+
+// x64 -> t64 = -1/2 K_oe x64 over all slots with the update's links and shape, `reps` launches
+// after one warm-up; returns the CUDA-event time of the reps on the engine stream.
+template <class LDT>
+static float time_update_hop_impl(wl_engine* E, cudaStream_t st, const Tune& t, int reps, const LDT& LD) {
+  using SFD = SpinorField<P_DOUBLE>;
+  HopArgs<LDT, SFD, EpiXpay<SFD, false>> A{};
+  A.g = E->ctx->g;
+  A.links = LD;
+  sf2<P_DOUBLE>(E->x64, A.src);
+  A.parity0 = 1;
+  A.nrhs = E->n;
+  A.mask = nullptr;
+  sf2<P_DOUBLE>(E->t64, A.epi.out);
+  A.epi.has_self = 0;
+  A.epi.b = E->neg_half;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  launch_hop<false, IdxCompact>(t, A, 1, st);
+  cudaEventRecord(e0, st);
+  for (int i = 0; i < reps; ++i) launch_hop<false, IdxCompact>(t, A, 1, st);
+  cudaEventRecord(e1, st);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms;
+}
+
+static float time_update_hop(wl_engine* E, cudaStream_t st, const Tune& t, int reps) {
+  if (E->ru_links12) return time_update_hop_impl(E, st, t, reps, LinkField<L_D12>{E->gauge->d12, E->ctx->g.Vh});
+  return time_update_hop_impl(E, st, t, reps, LinkField<L_D18>{E->gauge->d18, E->ctx->g.Vh});
+}
+
+extern "C" wl_status wl_engine_time_update_hop(wl_engine* E, int reps, double* ms, double* bytes) {
+  if (!E || !ms || !bytes || reps <= 0) WL_FAIL(nullptr, WL_ERR_ARG, "bad argument");
+  wl_ctx* ctx = E->ctx;
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  const float t = time_update_hop(E, engine_stream(E), E->td, reps);
+  wl_status s = check_launch(ctx, "wl_engine_time_update_hop");
+  if (s != WL_OK) return s;
+  *ms = (double)t / reps;
+  const double L = E->ru_links12 ? 96.0 : 144.0;
+  *bytes = (double)ctx->g.Vh * (8.0 * L + E->n * 2.0 * 192.0);
   return WL_OK;
 }
 
