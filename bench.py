@@ -501,6 +501,18 @@ def run_profile_dslash(args):
     ctx = L.WilsonContext(SHAPE, bc=BC, device=dev)
     U, eta = make_inputs(torch, dev, seed=0)
     gauge = ctx.gauge(U)
+    if args.dslash_layout == "update":  # the FP64 hop of the reliable update of the 16-slot FP16 engine
+        del U, eta
+        eng = L.Engine(ctx, gauge, NRHS, op="eo_normal", inner="half", tol=TOL, maxiter=10)
+        eng.time_hop(reps=3, update=True)
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()
+        ms, byts = eng.time_hop(reps=args.profile_dslash, update=True)
+        torch.cuda.cudart().cudaProfilerStop()
+        eng.close()
+        print(json.dumps({"profile": f"FP64 reliable-update hop, {NRHS} RHS in lanes", "shape": SHAPE, "ms": ms,
+                          "GBps": byts / ms / 1e6}), flush=True)
+        return
     if args.dslash_layout == "internal":  # the EO hop of the FP64 1-RHS engine (SoA fields, 18-real links)
         del U, eta
         eng = L.Engine(ctx, gauge, 1, op="eo_normal", inner="double", tol=TOL, maxiter=10)
@@ -594,8 +606,9 @@ def main():
                          "16 RHS (measured with --fp64-all)")
     ap.add_argument("--profile-dslash", type=int, default=0,
                     help="profiling driver: this many FP64 Dslash applications (on --shape)")
-    ap.add_argument("--dslash-layout", default="reference", choices=["reference", "internal"],
-                    help="--profile-dslash: reference-layout D, or the internal-layout EO hop")
+    ap.add_argument("--dslash-layout", default="reference", choices=["reference", "internal", "update"],
+                    help="--profile-dslash: reference-layout D, the internal-layout EO hop, or the FP64 "
+                         "reliable-update hop of the 16-slot engine")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -335,6 +335,14 @@ extern "C" wl_status wl_ctx_create(const wl_geometry* geom, int device, wl_ctx**
   g.fd_lth = make_fastdiv((unsigned)g.Lth);
   g.fd_l2 = make_fastdiv((unsigned)g.L[2]);
   g.fd_l1 = make_fastdiv((unsigned)g.L[1]);
+  g.Ty = 1;
+  for (int d = 8; d >= 1; --d)
+    if (g.L[1] % d == 0) {
+      g.Ty = d;
+      break;
+    }
+  g.fd_ty = make_fastdiv((unsigned)g.Ty);
+  g.fd_l0 = make_fastdiv((unsigned)g.L[0]);
   for (int mu = 0; mu < 4; ++mu) {
     g.ph_re[mu] = geom->bc_re[mu];
     g.ph_im[mu] = geom->bc_im[mu];

@@ -93,6 +93,8 @@ struct Geom {
   double ph_re[4], ph_im[4];  // boundary phase per direction
   int ph_on[4];               // phase != 1
   FastDiv fd_lth, fd_l2, fd_l1;  // divisions by Lt/2, Lz, Ly in the compact-index decomposition
+  int Ty;                         // y-slab width of the tiled sweep order (a divisor of Ly, <= 8)
+  FastDiv fd_ty, fd_l0;           // divisions by Ty and Lx
 };
 
 struct Site {
@@ -100,6 +102,25 @@ struct Site {
   int row;     // (x*Ly+y)*Lz+z
   int x[4];    // coordinates
 };
+
+// Tiled sweep order for kernels whose blocks walk the compact sites in order: the
+// logical index enumerates rows as (y-slab, x, y in slab, z) instead of (x, y, z),
+// so the x-neighbour rows of a row are Ty*Lz rows away in the sweep (not Ly*Lz)
+// and a source row's eight readers fall inside a window that stays in L2 even
+// for 16 FP64 RHS per site; a source row at a slab face is read once more by the
+// next slab.  Returns the compact index of logical position cl.
+WL_D int tiled_compact(const Geom& g, int cl) {
+  const int row_l = (int)fdiv(g.fd_lth, (unsigned)cl);
+  const int th = cl - row_l * g.Lth;
+  const int r1 = (int)fdiv(g.fd_l2, (unsigned)row_l);
+  const int z = row_l - r1 * g.L[2];
+  const int r2 = (int)fdiv(g.fd_ty, (unsigned)r1);
+  const int yi = r1 - r2 * g.Ty;
+  const int yb = (int)fdiv(g.fd_l0, (unsigned)r2);
+  const int x = r2 - yb * g.L[0];
+  const int row = (x * g.L[1] + yb * g.Ty + yi) * g.L[2] + z;
+  return row * g.Lth + th;
+}
 
 WL_D Site site_from_compact(const Geom& g, int parity, int c) {
   Site s;

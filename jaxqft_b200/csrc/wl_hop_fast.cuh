@@ -471,6 +471,7 @@ struct LaneSmemD {
   SiteLinksD link[S];
   int nb[S][8];
   int ok[S];
+  int c[S];  // compact index of each site (tiled sweep order)
 };
 
 // h = (1 + C g_mu) psi(nb) rows 0,1 (mu = 3 without its factor 2, applied by the
@@ -563,8 +564,9 @@ __global__ void __launch_bounds__(kLaneBlock, WL_LANE_D_MIN_BLOCKS) hop_lanes_d_
   const int wsite = (tid >> 5) * SPW;
   for (int j = tid & 31; j < 8 * SPW; j += 32) {
     const int sl = wsite + (j >> 3), q = j & 7, mu = q >> 1, dir = q & 1;
-    const int c = site0 + sl;
-    if (c < A.g.Vh) {
+    const int cl = site0 + sl;
+    if (cl < A.g.Vh) {
+      const int c = tiled_compact(A.g, cl);
       const Site s = site_from_compact(A.g, parity, c);
       const int nb = neighbor(A.g, s, mu, dir == 0 ? +1 : -1);
       Link<double> u;
@@ -579,14 +581,16 @@ __global__ void __launch_bounds__(kLaneBlock, WL_LANE_D_MIN_BLOCKS) hop_lanes_d_
 #pragma unroll
       for (int k = 0; k < 9; ++k) sm.link[sl].m[q][k] = make_double2(u.m[k / 3][k % 3].re, u.m[k / 3][k % 3].im);
       sm.nb[sl][q] = nb;
-      if (q == 0) sm.ok[sl] = 1;
+      if (q == 0) {
+        sm.ok[sl] = 1;
+        sm.c[sl] = c;
+      }
     } else if (q == 0) {
       sm.ok[sl] = 0;
     }
   }
   __syncwarp();
   const int sl = tid / R;
-  const int c = site0 + sl;
   const int rhs = blockIdx.y * R + (tid % R);
   double red = 0.0;
   const bool act = sm.ok[sl] && rhs < A.nrhs && (A.mask == nullptr || A.mask[rhs] != 0);
@@ -598,7 +602,7 @@ __global__ void __launch_bounds__(kLaneBlock, WL_LANE_D_MIN_BLOCKS) hop_lanes_d_
     lane_dir_d<1, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
     lane_dir_d<2, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
     lane_dir_d<3, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
-    red = A.epi(rhs, parity, (long long)c, acc);
+    red = A.epi(rhs, parity, (long long)sm.c[sl], acc);
   }
   if (EPI::kReduce) reduce_lanes<R>(red, A.red, A.nrhs, A.mask);
 }
