@@ -1663,6 +1663,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   E->h_maxiter.assign(n, E->prm.maxiter);
   E->ts = pick_tune(E, st);
   E->td = Tune{1, 128, 1};
+  E->td.pair = 1;  // FP64 fields site-major: the two-threads-per-site stencil
   if (E->lanes_mode) E->td = pick_update_tune(E, st);
   E->tsite = Tune{1, 128, 1};
   e = cudaStreamSynchronize(st);
