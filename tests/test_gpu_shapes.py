@@ -122,3 +122,34 @@ def test_fp64_stencil_shapes(setup, forced, nslots):
         ax = W.schur_even(U, s, masses[r], bc, normalized=True, dag=True)[0]
         assert np.linalg.norm(b[r] - ax) / np.linalg.norm(b[r]) <= 1e-10, (forced, r)
     eng.close()
+
+
+@pytest.fixture
+def forced_update(request):
+    os.environ["WL_FORCE_UPDATE_TUNE"] = request.param
+    yield request.param
+    del os.environ["WL_FORCE_UPDATE_TUNE"]
+
+
+@pytest.mark.parametrize("forced_update", ["16", "8", "4"], indirect=True)
+def test_update_hop_shapes(setup, forced_update):
+    """Every shape of the FP64 reliable-update hop (RHS lanes per sweep) gives solves
+    that reach the FP64 true-residual tolerance, checked against the oracle operator."""
+    shape, U, bc, ctx, gauge, rng = setup
+    n = 13
+    masses = np.linspace(-0.3, 0.1, n)
+    b = W.project(W.gaussian_spinor(rng, shape, n), 0)
+    eng = Engine(ctx, gauge, n, op="eo_normal", inner="half", tol=1e-10, maxiter=3000)
+    eng.admit(np.arange(n), torch.from_numpy(b), masses)
+    na = n
+    while na:
+        eng.step(8)
+        _, na = eng.poll()
+    for r in range(n):
+        x, st = eng.retire(r)
+        assert st["status"] == 2, (forced_update, r, st)
+        x = x.cpu().numpy()
+        s = W.schur_even(U, x[None], masses[r], bc, normalized=True)
+        ax = W.schur_even(U, s, masses[r], bc, normalized=True, dag=True)[0]
+        assert np.linalg.norm(b[r] - ax) / np.linalg.norm(b[r]) <= 1e-10, (forced_update, r)
+    eng.close()
