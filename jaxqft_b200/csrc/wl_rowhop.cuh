@@ -49,7 +49,7 @@ WL_D bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// global -> shared bulk copy completing on `bar` (no multicast)
+// global -> shared bulk copy into this CTA's own shared memory, completing on `bar`
 WL_D void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
   unsigned long long gsrc;
   asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(gsrc) : "l"(src));
@@ -58,7 +58,8 @@ WL_D void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long lon
                "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
-// 2D tensor-map global -> shared copy (box defined by the map), completing on `bar` (no multicast)
+// 2D tensor-map global -> shared copy (box defined by the map) into this CTA's own shared memory,
+// completing on `bar`
 WL_D void tma_g2s_2d(void* dst, const CUtensorMap* map, int c0, int c1, unsigned long long* bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
