@@ -243,6 +243,8 @@ class WilsonContext:
             raise ValueError(f"field of {psi.numel()} elements does not match lattice {self.lattice_shape}")
         if out is None:
             out = torch.empty_like(psi)
+        if nrhs == 0:  # an empty batch maps to an empty result, as the reference's vmapped operators do
+            return out
         flags = FLAG_NORMALIZED if normalized else 0
         self._check(self.lib.wl_apply(self.handle, gauge.handle, OPS[op], float(mass), flags, _ptr(psi), _ptr(out),
                                       nrhs))
@@ -350,6 +352,8 @@ class WilsonContext:
         p.use_x0 = int(x0 is not None)
         p.use_graph = int(bool(use_graph))
         p.check_every = int(check_every)
+        if nrhs == 0:  # nothing to solve: empty solution, no stats
+            return x, []
         stats = (WLSolveStats * nrhs)()
         rc = self.lib.wl_solve(self.handle, gauge.handle, ctypes.byref(p),
                                masses.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _ptr(b), _ptr(x), nrhs, stats)

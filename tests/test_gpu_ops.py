@@ -178,6 +178,26 @@ def test_batched_solve_masks_converged_rhs(setup):
         assert rel(x[r], _np(xs)) < 1e-8
 
 
+def test_empty_batch_returns_empty(setup):
+    """A batch of zero fields gives an empty result (the reference's vmapped
+    operators and solvers do the same), launches nothing and leaves the
+    context usable."""
+    from jaxqft_b200 import lib as L
+
+    g, ctx, gauges = setup
+    shape = tuple(int(v) for v in g["shape"])
+    m = float(g["mass"])
+    empty = torch.zeros((0, *shape, 4, 3), dtype=torch.complex128, device="cuda")
+    n0 = L.kernel_launches()
+    out = ctx.apply("D", gauges[0], m, empty)
+    x, st = ctx.solve(gauges[0], empty, m, op="eo_normal", tol=1e-10, inner="half")
+    assert out.shape == empty.shape and x.shape == empty.shape and st == []
+    assert L.kernel_launches() == n0
+    psi = W.gaussian_spinor(np.random.default_rng(5), shape, 1)
+    d = _np(ctx.apply("D", gauges[0], m, torch.from_numpy(psi)))
+    assert rel(d, W.apply_D(g["U"][:1], psi, m, g["bc"])) < OP_TOL
+
+
 def test_anisotropic_lattice_against_oracle():
     shape = (4, 6, 2, 8)
     rng = np.random.default_rng(21)
