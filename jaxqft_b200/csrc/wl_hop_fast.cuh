@@ -235,10 +235,12 @@ __global__ void __launch_bounds__(256) hop_fast_kernel(HopArgs<LF, SF, EPI> A) {
 // one 32-byte sector.
 constexpr int kLaneBlock = 128;
 // Resident blocks per SM the FP32-arithmetic lane kernel is compiled for:
-// 8 caps it at 64 registers (32 warps per SM) to hide the L2 latency of the
-// neighbour gathers.
+// 7 caps it at 72 registers (28 warps per SM), enough warps to hide the L2
+// latency of the neighbour gathers.  Measured at 24^3x48 with 16 FP16 RHS
+// (whole batched solve, interleaved runs): 7 blocks 348.5-349.0 ms, 8 blocks
+// (64 registers) 350.0-350.5 ms, 6 blocks (80 registers) 357.5 ms.
 #ifndef WL_LANE_MIN_BLOCKS
-#define WL_LANE_MIN_BLOCKS 8
+#define WL_LANE_MIN_BLOCKS 7
 #endif
 
 struct LinkSmem {
