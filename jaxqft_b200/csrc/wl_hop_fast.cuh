@@ -234,14 +234,36 @@ __global__ void __launch_bounds__(256) hop_fast_kernel(HopArgs<LF, SF, EPI> A) {
 // sector-efficient: lanes r of sites c and c+1 read the two 16-byte halves of
 // one 32-byte sector.
 constexpr int kLaneBlock = 128;
-// Resident blocks per SM the FP32-arithmetic lane kernel is compiled for:
-// 7 caps it at 72 registers (28 warps per SM), enough warps to hide the L2
-// latency of the neighbour gathers.  Measured at 24^3x48 with 16 FP16 RHS
-// (whole batched solve, interleaved runs): 7 blocks 348.5-349.0 ms, 8 blocks
-// (64 registers) 350.0-350.5 ms, 6 blocks (80 registers) 357.5 ms.
+// Resident blocks per SM the FP32-arithmetic lane kernel is compiled for,
+// per epilogue: 7 (72 registers, 28 warps per SM) for K_oe p and the fused
+// CG hop, 8 (64 registers, 32 warps) for the reducing xpay hop (M p with
+// |Mp|^2) and the plain dagger hop (K^dag_oe y).  Enough warps hide the L2
+// latency of the neighbour gathers; more registers cut spill and
+// rematerialisation work.  Measured at 24^3x48 with 16 FP16 RHS (whole
+// batched solve, interleaved runs): this split 344.6-346.2 ms, 7 blocks for
+// all four 346.9-347.6 ms; on another box 7 blocks for all 348.5-349.0 ms,
+// 8 blocks for all 350.0-350.5 ms, 6 blocks for all 357.5 ms.
 #ifndef WL_LANE_MIN_BLOCKS
 #define WL_LANE_MIN_BLOCKS 7
 #endif
+#ifndef WL_LANE_MIN_BLOCKS_XPAY_RED
+#define WL_LANE_MIN_BLOCKS_XPAY_RED 8
+#endif
+#ifndef WL_LANE_MIN_BLOCKS_DAG_XPAY
+#define WL_LANE_MIN_BLOCKS_DAG_XPAY 8
+#endif
+template <bool DAG, class EPI>
+struct LaneMinBlocks {
+  static constexpr int value = WL_LANE_MIN_BLOCKS;
+};
+template <bool DAG, class SF>
+struct LaneMinBlocks<DAG, EpiXpay<SF, true>> {
+  static constexpr int value = WL_LANE_MIN_BLOCKS_XPAY_RED;
+};
+template <class SF>
+struct LaneMinBlocks<true, EpiXpay<SF, false>> {
+  static constexpr int value = WL_LANE_MIN_BLOCKS_DAG_XPAY;
+};
 
 struct LinkSmem {
   float4 p[9];  // (R.x, R.y, I.x, I.y) for element (a, b) = k / 3, k % 3
@@ -388,7 +410,7 @@ WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* /*mask*/
 }
 
 template <bool DAG, int R, class LF, class SF, class EPI>
-__global__ void __launch_bounds__(kLaneBlock, WL_LANE_MIN_BLOCKS) hop_lanes_kernel(HopArgs<LF, SF, EPI> A) {
+__global__ void __launch_bounds__(kLaneBlock, LaneMinBlocks<DAG, EPI>::value) hop_lanes_kernel(HopArgs<LF, SF, EPI> A) {
   constexpr int S = kLaneBlock / R;
   __shared__ LaneSmem<R> sm;
   const int tid = threadIdx.x;
