@@ -76,7 +76,11 @@ typedef struct wl_engine wl_engine;
 int wl_version(void);
 /* Create a context for one lattice geometry on CUDA device `device`.
    Replaces the geometry set-up of SU3WilsonNf2.__post_init__
-   (jaxqft/models/su3_wilson_nf2.py:625-709: BC factor, masks, EO maps). */
+   (jaxqft/models/su3_wilson_nf2.py:625-709: BC factor, masks, EO maps).
+   Every extent must be even and >= 2, else WL_ERR_ARG.  The reference
+   accepts odd extents, but there a wrap by one site keeps the parity, so its
+   EO neighbour maps (su3_wilson_nf2.py:847-882) hold -1 entries and its EO
+   operators and solvers are not defined; only its unpreconditioned D is. */
 wl_status wl_ctx_create(const wl_geometry* geom, int device, wl_ctx** out);
 void wl_ctx_destroy(wl_ctx* ctx);
 const char* wl_last_error(const wl_ctx* ctx);
