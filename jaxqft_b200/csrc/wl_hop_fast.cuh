@@ -242,7 +242,9 @@ constexpr int kLaneBlock = 128;
 // rematerialisation work.  Measured at 24^3x48 with 16 FP16 RHS (whole
 // batched solve, interleaved runs): this split 344.6-346.2 ms, 7 blocks for
 // all four 346.9-347.6 ms; on another box 7 blocks for all 348.5-349.0 ms,
-// 8 blocks for all 350.0-350.5 ms, 6 blocks for all 357.5 ms.
+// 8 blocks for all 350.0-350.5 ms, 6 blocks for all 357.5 ms; on a third box
+// this split 351.8-352.9 ms, 6 blocks (80 registers) for the CG hop alone or
+// for K_oe p alone 356.2-357.0 ms.  Each cap can be overridden with -D.
 #ifndef WL_LANE_MIN_BLOCKS
 #define WL_LANE_MIN_BLOCKS 7
 #endif
@@ -252,6 +254,14 @@ constexpr int kLaneBlock = 128;
 #ifndef WL_LANE_MIN_BLOCKS_DAG_XPAY
 #define WL_LANE_MIN_BLOCKS_DAG_XPAY 8
 #endif
+#ifndef WL_LANE_MIN_BLOCKS_CG
+#define WL_LANE_MIN_BLOCKS_CG WL_LANE_MIN_BLOCKS
+#endif
+#ifndef WL_LANE_MIN_BLOCKS_XPAY
+#define WL_LANE_MIN_BLOCKS_XPAY WL_LANE_MIN_BLOCKS
+#endif
+template <class SF>
+struct EpiCG;  // wl_site.cuh
 template <bool DAG, class EPI>
 struct LaneMinBlocks {
   static constexpr int value = WL_LANE_MIN_BLOCKS;
@@ -263,6 +273,14 @@ struct LaneMinBlocks<DAG, EpiXpay<SF, true>> {
 template <class SF>
 struct LaneMinBlocks<true, EpiXpay<SF, false>> {
   static constexpr int value = WL_LANE_MIN_BLOCKS_DAG_XPAY;
+};
+template <class SF>
+struct LaneMinBlocks<false, EpiXpay<SF, false>> {
+  static constexpr int value = WL_LANE_MIN_BLOCKS_XPAY;
+};
+template <bool DAG, class SF>
+struct LaneMinBlocks<DAG, EpiCG<SF>> {
+  static constexpr int value = WL_LANE_MIN_BLOCKS_CG;
 };
 
 struct LinkSmem {
