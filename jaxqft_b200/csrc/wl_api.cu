@@ -15,6 +15,7 @@
 #include <type_traits>
 
 #include <cudaTypedefs.h>
+#include <nvtx3/nvToolsExt.h>
 #include <vector>
 
 #include "../../include/wilson_sm100.h"
@@ -26,6 +27,16 @@
 #include "wl_site.cuh"
 
 using namespace wl;
+
+// Named host ranges around the entry points (NVTX, header-only and inert
+// unless a profiler is attached).  A tool can then attribute kernels to the
+// call that launched them, e.g. ncu --nvtx --nvtx-include "wl_solve/".
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // ============================================================== error helpers
 struct wl_ctx {
@@ -432,6 +443,7 @@ static wl_status gauge_fill(wl_gauge* G, const void* U) {
 }
 
 extern "C" wl_status wl_gauge_create(wl_ctx* ctx, const void* U, wl_gauge** out) {
+  NvtxRange nvtx_range("wl_gauge_create");
   if (!ctx || !U || !out) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
   WL_CUDA(ctx, cudaSetDevice(ctx->device));
   const Geom& g = ctx->g;
@@ -461,6 +473,7 @@ extern "C" wl_status wl_gauge_create(wl_ctx* ctx, const void* U, wl_gauge** out)
 }
 
 extern "C" wl_status wl_gauge_update(wl_gauge* G, const void* U) {
+  NvtxRange nvtx_range("wl_gauge_update");
   if (!G || !U) WL_FAIL(nullptr, WL_ERR_ARG, "null argument");
   return gauge_fill(G, U);
 }
@@ -618,6 +631,7 @@ static void ref_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const v
 
 extern "C" wl_status wl_apply(wl_ctx* ctx, wl_gauge* G, int op, double mass, unsigned flags, const void* in, void* out,
                               int nrhs) {
+  NvtxRange nvtx_range("wl_apply");
   if (!ctx || !G || !in || !out) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
   if (in == out) WL_FAIL(ctx, WL_ERR_ARG, "in and out must not alias");
   if (nrhs <= 0) WL_FAIL(ctx, WL_ERR_ARG, "nrhs must be positive");
@@ -693,6 +707,7 @@ extern "C" wl_status wl_apply(wl_ctx* ctx, wl_gauge* G, int op, double mass, uns
 // ============================================================== force
 extern "C" wl_status wl_pf_force(wl_ctx* ctx, wl_gauge* G, const void* X, const void* Y, double coef, int accumulate,
                                  void* F) {
+  NvtxRange nvtx_range("wl_pf_force");
   if (!ctx || !G || !X || !Y || !F) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
   WL_CUDA(ctx, cudaSetDevice(ctx->device));
   const Geom& g = ctx->g;
@@ -753,6 +768,7 @@ static GaugeArgs gauge_args(wl_ctx* ctx, const void* U, const void* P, void* out
 }
 
 extern "C" wl_status wl_gauge_force(wl_ctx* ctx, const void* U, int batch, double beta, void* F) {
+  NvtxRange nvtx_range("wl_gauge_force");
   if (!ctx || !U || !F || batch < 1) WL_FAIL(ctx, WL_ERR_ARG, "null argument or batch < 1");
   WL_CUDA(ctx, cudaSetDevice(ctx->device));
   GaugeArgs A = gauge_args(ctx, U, nullptr, F, batch, -beta / 3.0);
@@ -763,6 +779,7 @@ extern "C" wl_status wl_gauge_force(wl_ctx* ctx, const void* U, int batch, doubl
 }
 
 extern "C" wl_status wl_gauge_evolve(wl_ctx* ctx, const void* P, const void* U, int batch, double dt, void* Uout) {
+  NvtxRange nvtx_range("wl_gauge_evolve");
   if (!ctx || !P || !U || !Uout || batch < 1) WL_FAIL(ctx, WL_ERR_ARG, "null argument or batch < 1");
   WL_CUDA(ctx, cudaSetDevice(ctx->device));
   GaugeArgs A = gauge_args(ctx, U, P, Uout, batch, dt);
@@ -773,6 +790,7 @@ extern "C" wl_status wl_gauge_evolve(wl_ctx* ctx, const void* P, const void* U, 
 }
 
 extern "C" wl_status wl_gauge_plaquette_sum(wl_ctx* ctx, const void* U, int batch, double* plaq_sum) {
+  NvtxRange nvtx_range("wl_gauge_plaquette_sum");
   if (!ctx || !U || !plaq_sum || batch < 1) WL_FAIL(ctx, WL_ERR_ARG, "null argument or batch < 1");
   WL_CUDA(ctx, cudaSetDevice(ctx->device));
   const int nblk = (ctx->g.V + 127) / 128;
@@ -787,6 +805,7 @@ extern "C" wl_status wl_gauge_plaquette_sum(wl_ctx* ctx, const void* U, int batc
 }
 
 extern "C" wl_status wl_momentum_kinetic(wl_ctx* ctx, const void* P, int batch, double* kin) {
+  NvtxRange nvtx_range("wl_momentum_kinetic");
   if (!ctx || !P || !kin || batch < 1) WL_FAIL(ctx, WL_ERR_ARG, "null argument or batch < 1");
   WL_CUDA(ctx, cudaSetDevice(ctx->device));
   const int nblk = (int)((4LL * ctx->g.V + 127) / 128);
@@ -801,6 +820,7 @@ extern "C" wl_status wl_momentum_kinetic(wl_ctx* ctx, const void* P, int batch, 
 }
 
 extern "C" wl_status wl_pion_correlator(wl_ctx* ctx, const void* prop, int ncol, int source_t, double* corr) {
+  NvtxRange nvtx_range("wl_pion_correlator");
   if (!ctx || !prop || !corr || ncol < 1) WL_FAIL(ctx, WL_ERR_ARG, "null argument or ncol < 1");
   WL_CUDA(ctx, cudaSetDevice(ctx->device));
   const Geom& g = ctx->g;
@@ -1565,6 +1585,7 @@ extern "C" void wl_engine_destroy(wl_engine* E) {
 
 extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_params* prm, int nslots,
                                       wl_engine** out) {
+  NvtxRange nvtx_range("wl_engine_create");
   if (!ctx || !G || !prm || !out) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
   if (nslots <= 0 || nslots > 4096) WL_FAIL(ctx, WL_ERR_ARG, "nslots out of range");
   if (prm->op != WL_SOLVE_NORMAL && prm->op != WL_SOLVE_EO_NORMAL) WL_FAIL(ctx, WL_ERR_ARG, "unknown solve op");
@@ -1724,6 +1745,7 @@ static wl_status admit_impl(wl_engine* E, const int* slots, int nadm, const void
 
 extern "C" wl_status wl_engine_admit(wl_engine* E, const int* slots, int nadm, const void* b, const double* masses,
                                      const double* tols, const int* maxiters) {
+  NvtxRange nvtx_range("wl_engine_admit");
   return admit_impl(E, slots, nadm, b, nullptr, masses, tols, maxiters);
 }
 
@@ -1811,6 +1833,7 @@ static wl_status build_graph(wl_engine* E, cudaStream_t st) {
 }
 
 extern "C" wl_status wl_engine_step(wl_engine* E, int iters) {
+  NvtxRange nvtx_range("wl_engine_step");
   if (!E) WL_FAIL(nullptr, WL_ERR_ARG, "null engine");
   wl_ctx* ctx = E->ctx;
   WL_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -1975,6 +1998,7 @@ static wl_status engine_unpack(wl_engine* E, int first, int count, void* x) {
 }
 
 extern "C" wl_status wl_engine_retire(wl_engine* E, int slot, void* x, wl_solve_stats* stats) {
+  NvtxRange nvtx_range("wl_engine_retire");
   if (!E || !x) WL_FAIL(nullptr, WL_ERR_ARG, "null argument");
   if (slot < 0 || slot >= E->n) WL_FAIL(E->ctx, WL_ERR_ARG, "slot index out of range");
   wl_status s = engine_unpack(E, slot, 1, x);
@@ -2005,6 +2029,7 @@ static std::mutex g_solve_mu;
 
 extern "C" wl_status wl_solve(wl_ctx* ctx, wl_gauge* G, const wl_solve_params* prm, const double* masses,
                               const void* b, void* x, int nrhs, wl_solve_stats* stats) {
+  NvtxRange nvtx_range("wl_solve");
   if (!ctx || !G || !prm || !masses || !b || !x) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
   if (nrhs <= 0) WL_FAIL(ctx, WL_ERR_ARG, "nrhs must be positive");
   wl_engine* E = nullptr;
