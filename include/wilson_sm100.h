@@ -184,6 +184,15 @@ wl_status wl_engine_debug_apply(wl_engine* eng, int stage, double mass, const vo
    (graph launches count every kernel node of the graph). */
 int64_t wl_kernel_launches(void);
 
+/* Checking builds (no counterpart in the reference; compiled with
+   -DWL_BOUNDS_CHECK=1 as libwilson_sm100_check.so): the kernels compare every
+   compact site index they decode or gather with the half volume, count the
+   ones out of range, keep the first and use site 0 instead, so the access
+   stays in bounds.  Returns the count on the current device since the last
+   call and clears it (after a device synchronisation), with the first bad
+   index in *first_bad; -1 in a build without the checks, -2 on a CUDA error. */
+int64_t wl_bounds_errors(long long* first_bad);
+
 /* Allocation-free operator (no counterpart in the reference) -------------- */
 /* out = S_e^dag S_e in, exactly what wl_apply(WL_OP_SCHUR_E_NORMAL) computes,
    for callers that cannot call cudaMalloc: a JAX/XLA custom-call handler

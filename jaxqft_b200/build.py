@@ -1,6 +1,7 @@
 """Build libwilson_sm100.so in-tree with nvcc for sm_100a.
 
-    python -m jaxqft_b200.build        (or jaxqft_b200.build.build())
+    python -m jaxqft_b200.build          (or jaxqft_b200.build.build())
+    python -m jaxqft_b200.build --check  (libwilson_sm100_check.so, device-side index checks)
 
 The library is written next to this file so that it travels with the source
 tree; nothing is installed into site-packages.
@@ -37,32 +38,72 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found; the CUDA toolkit is required to build libwilson_sm100.so")
 
 
-def _stale() -> bool:
-    if not os.path.exists(LIB):
+CHECK_LIB = os.path.join(HERE, "libwilson_sm100_check.so")
+CHECK_DEFINES = ["-DWL_BOUNDS_CHECK=1"]  # device-side index checks (see wl_common.cuh)
+
+
+def _stale(lib: str = LIB) -> bool:
+    if not os.path.exists(lib):
         return True
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(INCLUDE, "wilson_sm100.h")]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+def _nvcc_cmd(lib: str, extra=()) -> list:
+    return [nvcc(), *NVCC_FLAGS, *extra, "-I", INCLUDE, "-o", lib + ".tmp"] + [os.path.join(CSRC, f) for f in SOURCES]
+
+
+def _finish(lib: str, res_code: int, out: str, verbose: bool) -> str:
+    if res_code != 0:
+        sys.stderr.write(out)
+        raise RuntimeError(f"nvcc failed building {os.path.basename(lib)}")
+    if verbose and out:
+        sys.stderr.write(out)
+    os.replace(lib + ".tmp", lib)
+    return lib
+
+
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
-    if not force and not _stale():
+    """The release library libwilson_sm100.so."""
+    if not force and not _stale(LIB):
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", INCLUDE, "-o", LIB + ".tmp"]
-    cmd += [os.path.join(CSRC, f) for f in SOURCES]
+    cmd = _nvcc_cmd(LIB, extra)
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building libwilson_sm100.so")
-    if verbose and res.stderr:
-        sys.stderr.write(res.stderr)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    return _finish(LIB, res.returncode, res.stdout + res.stderr, verbose)
+
+
+def build_check(force: bool = False, verbose: bool = False) -> str:
+    """The checking library libwilson_sm100_check.so (same sources, WL_BOUNDS_CHECK=1)."""
+    if not force and not _stale(CHECK_LIB):
+        return CHECK_LIB
+    cmd = _nvcc_cmd(CHECK_LIB, CHECK_DEFINES)
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    return _finish(CHECK_LIB, res.returncode, res.stdout + res.stderr, verbose)
+
+
+def build_all(force: bool = False, verbose: bool = False) -> None:
+    """Both libraries, the two nvcc runs in parallel."""
+    jobs = []
+    for lib, extra in ((LIB, ()), (CHECK_LIB, CHECK_DEFINES)):
+        if force or _stale(lib):
+            cmd = _nvcc_cmd(lib, extra)
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            jobs.append((lib, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    for lib, proc in jobs:
+        out, _ = proc.communicate()
+        _finish(lib, proc.returncode, out, verbose)
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True,
-          extra=(["-Xptxas", "-v"] if "--ptxas-v" in sys.argv else []))
-    print(LIB)
+    if "--check" in sys.argv:
+        print(build_check(force="--force" in sys.argv, verbose=True))
+    else:
+        build(force="--force" in sys.argv, verbose=True,
+              extra=(["-Xptxas", "-v"] if "--ptxas-v" in sys.argv else []))
+        print(LIB)

@@ -73,6 +73,31 @@ static thread_local std::string g_static_err;
 static std::atomic<long long> g_launches{0};
 extern "C" int64_t wl_kernel_launches(void) { return g_launches.load(); }
 
+// Out-of-range site indices counted by a checking build on the current device
+// since the last call (and cleared), or -1 in a build without the checks.
+extern "C" int64_t wl_bounds_errors(long long* first_bad) {
+#if WL_BOUNDS_CHECK
+  unsigned int n = 0;
+  long long first = 0;
+  if (cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpyFromSymbol(&n, g_wl_bounds_errors, sizeof(n)) != cudaSuccess ||
+      cudaMemcpyFromSymbol(&first, g_wl_bounds_first, sizeof(first)) != cudaSuccess) {
+    cudaGetLastError();
+    return -2;
+  }
+  const unsigned int zero = 0;
+  if (cudaMemcpyToSymbol(g_wl_bounds_errors, &zero, sizeof(zero)) != cudaSuccess) {
+    cudaGetLastError();
+    return -2;
+  }
+  if (first_bad) *first_bad = first;
+  return (int64_t)n;
+#else
+  if (first_bad) *first_bad = 0;
+  return -1;
+#endif
+}
+
 static inline void set_err(wl_ctx* ctx, const std::string& m);
 #define WL_FAIL(ctx, code, msg) \
   do {                          \

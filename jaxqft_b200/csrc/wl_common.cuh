@@ -103,6 +103,29 @@ struct Site {
   int x[4];    // coordinates
 };
 
+// Checking build (-DWL_BOUNDS_CHECK=1): every compact site index that the
+// decode, the tiled sweep and the neighbour gathers produce is compared with
+// Vh.  An index out of range is counted in g_wl_bounds_errors, the first one is
+// kept in g_wl_bounds_first, and 0 is used instead so the access stays inside
+// the field (no assert, no trap).  wl_bounds_errors() reads and clears the count.
+#ifndef WL_BOUNDS_CHECK
+#define WL_BOUNDS_CHECK 0
+#endif
+#if WL_BOUNDS_CHECK
+__device__ unsigned int g_wl_bounds_errors;
+__device__ long long g_wl_bounds_first;
+WL_D int wl_checked_index(long long v, long long n) {
+  if (v < 0 || v >= n) {
+    if (atomicAdd(&g_wl_bounds_errors, 1u) == 0u) g_wl_bounds_first = v;
+    return 0;
+  }
+  return (int)v;
+}
+#define WL_CHECKED(v, n) wl_checked_index((long long)(v), (long long)(n))
+#else
+#define WL_CHECKED(v, n) (v)
+#endif
+
 // Tiled sweep order for kernels whose blocks walk the compact sites in order: the
 // logical index enumerates rows as (y-slab, x, y in slab, z) instead of (x, y, z),
 // so the x-neighbour rows of a row are Ty*Lz rows away in the sweep (not Ly*Lz)
@@ -119,11 +142,12 @@ WL_D int tiled_compact(const Geom& g, int cl) {
   const int yb = (int)fdiv(g.fd_l0, (unsigned)r2);
   const int x = r2 - yb * g.L[0];
   const int row = (x * g.L[1] + yb * g.Ty + yi) * g.L[2] + z;
-  return row * g.Lth + th;
+  return WL_CHECKED(row * g.Lth + th, g.Vh);
 }
 
 WL_D Site site_from_compact(const Geom& g, int parity, int c) {
   Site s;
+  c = WL_CHECKED(c, g.Vh);
   s.c = c;
   const int row = (int)fdiv(g.fd_lth, (unsigned)c);
   const int th = c - row * g.Lth;
@@ -141,13 +165,13 @@ WL_D int neighbor(const Geom& g, const Site& s, int mu, int dir) {
   if (mu == 3) {
     int t = s.x[3] + dir;
     t = (t < 0) ? t + g.L[3] : (t >= g.L[3] ? t - g.L[3] : t);
-    return s.row * g.Lth + (t >> 1);
+    return WL_CHECKED(s.row * g.Lth + (t >> 1), g.Vh);
   }
   int xm = s.x[mu] + dir;
   int row = s.row + dir * g.strideRow[mu];
   if (xm < 0) row += g.L[mu] * g.strideRow[mu];
   else if (xm >= g.L[mu]) row -= g.L[mu] * g.strideRow[mu];
-  return row * g.Lth + (s.x[3] >> 1);
+  return WL_CHECKED(row * g.Lth + (s.x[3] >> 1), g.Vh);
 }
 
 // ---------------------------------------------------------------- loads

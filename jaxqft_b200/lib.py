@@ -16,6 +16,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libwilson_sm100.so")
+# the same library compiled with device-side index checks (WL_BOUNDS_CHECK)
+CHECK_LIB_PATH = os.path.join(HERE, "libwilson_sm100_check.so")
 HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "wilson_sm100.h")
 
 # status codes (wl_status)
@@ -40,7 +42,7 @@ EXPORTS = (
     "wl_engine_step", "wl_engine_poll", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
     "wl_engine_stream", "wl_engine_time_hop", "wl_engine_time_update_hop", "wl_kernel_launches", "wl_engine_debug_apply",
     "wl_apply_schur_normal_noalloc", "wl_gauge_force", "wl_gauge_evolve", "wl_gauge_plaquette_sum",
-    "wl_momentum_kinetic", "wl_pion_correlator",
+    "wl_momentum_kinetic", "wl_pion_correlator", "wl_bounds_errors",
 )
 
 
@@ -106,6 +108,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wl_engine_time_hop": (i, [vp, i, pd, pd]),
         "wl_engine_time_update_hop": (i, [vp, i, pd, pd]),
         "wl_kernel_launches": (ctypes.c_int64, []),
+        "wl_bounds_errors": (ctypes.c_int64, [ctypes.POINTER(ctypes.c_longlong)]),
         "wl_engine_debug_apply": (i, [vp, i, d, vp, vp]),
         "wl_apply_schur_normal_noalloc": (i, [vp, vp, d, u, vp, vp, i]),
         "wl_gauge_force": (i, [vp, vp, i, d, vp]),

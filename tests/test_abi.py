@@ -38,3 +38,12 @@ def test_context_rejects_odd_extents_without_device_work():
     rc = lib.wl_ctx_create(ctypes.byref(g), 0, ctypes.byref(h))
     assert rc == L.WL_ERR_ARG
     assert b"even" in lib.wl_last_error(None)
+
+
+def test_release_build_reports_no_index_checks():
+    """wl_bounds_errors is -1 in the release library (the checks are compiled
+    only into libwilson_sm100_check.so); it makes no device call there."""
+    lib = L.load_library()
+    first = ctypes.c_longlong(7)
+    assert lib.wl_bounds_errors(ctypes.byref(first)) == -1
+    assert first.value == 0
