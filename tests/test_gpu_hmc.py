@@ -101,3 +101,25 @@ def test_energy_violation_scales_as_eps_squared(md_setup):
     d = [abs(_dH(th, U, P, nmd, 0.5)[0]) for nmd in (4, 8, 16)]
     slopes = [np.log2(d[i] / d[i + 1]) for i in range(2)]
     assert all(1.6 < s < 2.4 for s in slopes), (d, slopes)
+
+
+def test_identically_seeded_chains_are_bitwise_reproducible():
+    """Two HMC chains with the same seeds give bit-identical dH, decisions and
+    links (the reference's mcmc_smoke.py:148-200 allows 1e-7; the reductions
+    here have a fixed order and no floating-point atomics, so repeats agree
+    exactly)."""
+    shape, mass, bc = (4, 4, 4, 4), W.kappa_to_mass(0.13), (1, 1, 1, -1)
+    U0 = W.hot_links(np.random.default_rng(9), shape, 1, 0.1)
+
+    def chain():
+        th = SU3WilsonNf2(lattice_shape=shape, beta=5.6, mass=mass, fermion_bc=bc, cg_tol=1e-10, cg_maxiter=5000,
+                          fermion_monomial_kind="eo_preconditioned", pseudofermion_force_mode="analytic",
+                          solver_precision="half", seed=11)
+        hmc = HMC(th, MinNorm2(th.force, th.evolve_q, 4, 0.5), verbose=False, seed=12)
+        U = hmc.evolve(torch.from_numpy(U0).cuda(), 3)
+        return [(h["dH"][0], h["accepted"][0]) for h in hmc.history], U.cpu().numpy()
+
+    h1, U1 = chain()
+    h2, U2 = chain()
+    assert len(h1) == 3 and h1 == h2
+    assert np.array_equal(U1, U2)

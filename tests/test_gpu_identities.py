@@ -93,3 +93,28 @@ def test_gauge_covariance():
     th.set_loaded_pseudofermion(phip)
     s1 = float(th.fermion_monomial.action(Upt)[0])
     assert abs(s0 - s1) < 1e-9 * abs(s0), (s0, s1)
+
+
+@pytest.mark.parametrize("kind", ["unpreconditioned", "eo_preconditioned"])
+def test_force_gauge_covariance(kind):
+    """Pseudofermion force covariance (su3_wilson_nf2.py:2415-2469): with
+    U'_mu(x) = Om(x)^dag U_mu(x) Om(x+mu) and phi' = Om^dag phi, the analytic
+    force satisfies F_mu[U', phi'](x) = Om(x)^dag F_mu[U, phi](x) Om(x)."""
+    th = _theory(kind)
+    rng = np.random.default_rng(6)
+    U = W.hot_links(rng, SHAPE, 1, 0.3)
+    V = int(np.prod(SHAPE))
+    Om = _random_su3(rng, V).reshape(*SHAPE, 3, 3)
+    Od = np.conj(np.swapaxes(Om, -1, -2))
+    Up = np.empty_like(U)
+    for mu in range(4):
+        Up[0, mu] = Od @ U[0, mu] @ np.roll(Om, -1, axis=mu)
+    Ut = torch.from_numpy(U).cuda()
+    m = th.fermion_monomial
+    m.refresh(Ut)
+    phi = m.phi.cpu().numpy()
+    phip = np.einsum("...ab,n...sb->n...sa", Od, phi)  # site-local: odd sites of an even phi stay zero
+    F = m.force_analytic(Ut, torch.from_numpy(phi).cuda()).cpu().numpy()
+    Fp = m.force_analytic(torch.from_numpy(Up).cuda(), torch.from_numpy(phip).cuda()).cpu().numpy()
+    Fcov = np.stack([Od @ F[:, mu] @ Om for mu in range(4)], axis=1)
+    assert np.linalg.norm(Fp - Fcov) / np.linalg.norm(Fcov) < 1e-8
