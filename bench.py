@@ -40,6 +40,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from jaxqft_b200.wilson import WilsonDiracOperator  # noqa: E402  (pure Python: the flop counter)
+
+DIRAC = WilsonDiracOperator()
+
 SHAPE = (24, 24, 24, 48)
 KAPPA = 0.135
 MASS = 1.0 / (2.0 * KAPPA) - 4.0
@@ -254,6 +258,8 @@ def run_ours(args):
     dslash_native["frac"] = dslash_native["achieved"] / peaks()[0]
     dslash_native["peak"] = peaks()[0]
     dslash_native.update(naive_rate(np.prod(SHAPE) // 2, 1, 192, 144, n_ms))
+    dslash_native.update(ref_gflops(DIRAC.flops_per_site_dslash(3) * int(np.prod(SHAPE)) // 2, n_ms,
+                                    "flops_per_site_dslash x Vh"))
     eng64.close()
 
     # ---- live roofline of the dominant kernel (FP16 hop over 16 RHS)
@@ -277,11 +283,14 @@ def run_ours(args):
     ctx.synchronize()
     d_ms = e0.elapsed_time(e1) / 20
     d_bytes = float(np.prod(SHAPE)) * (4 * 144 + 2 * 192)  # 4 links + in/out spinor per site (FP64)
-    dslash = {"kernel": "D = m0 - hop/2, reference layout, FP64, 1 RHS (row-staged TMA bulk copies)",
+    dslash = {"kernel": "D = m0 - hop/2, reference layout, FP64, 1 RHS (ref_pair_kernel: two threads per site, "
+                        "256-bit spinor accesses, parity-split SoA links)",
               "ms_per_launch": d_ms, "algorithmic_bytes_per_launch": d_bytes,
               "achieved": d_bytes / (d_ms * 1e-3) / 1e9, "unit": "GB/s"}
     dslash["frac"] = dslash["achieved"] / peaks()[0]
+    dslash["peak"] = peaks()[0]
     dslash.update(naive_rate(np.prod(SHAPE), 1, 192, 144, d_ms))
+    dslash.update(ref_gflops(DIRAC.flops_per_matvec_call(3, int(np.prod(SHAPE))), d_ms, "flops_per_matvec_call"))
     del psi1, dout
 
     # ---- e2e through the public API from pinned host buffers: a stream of K
@@ -289,55 +298,53 @@ def run_ours(args):
     # of its 16 solutions; the copies of neighbouring steps run on a copy stream
     # while the solver runs (double-buffered), and the timed region (CUDA events
     # on the compute stream, after the copy stream drained) spans all K steps.
-    e2e = None
-    if rank == 0 or True:
-        b_host = [b.cpu().pin_memory(), b.cpu().pin_memory()]
-        x_host = [torch.empty_like(b_host[0]).pin_memory(), torch.empty_like(b_host[0]).pin_memory()]
-        b_dev = [torch.empty_like(b), torch.empty_like(b)]
-        cur = torch.cuda.current_stream(dev)
-        cps = torch.cuda.Stream(dev)
+    b_host = [b.cpu().pin_memory(), b.cpu().pin_memory()]
+    x_host = [torch.empty_like(b_host[0]).pin_memory(), torch.empty_like(b_host[0]).pin_memory()]
+    b_dev = [torch.empty_like(b), torch.empty_like(b)]
+    cur = torch.cuda.current_stream(dev)
+    cps = torch.cuda.Stream(dev)
 
-        def e2e_stream(K):
-            ev_in = [torch.cuda.Event(), torch.cuda.Event()]
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize(dev)
-            e0.record(cur)
-            cps.wait_event(e0)
-            with torch.cuda.stream(cps):
-                b_dev[0].copy_(b_host[0], non_blocking=True)
-                ev_in[0].record(cps)
-            last = None
-            for i in range(K):
-                cur.wait_event(ev_in[i % 2])
-                if i + 1 < K:
-                    with torch.cuda.stream(cps):
-                        b_dev[(i + 1) % 2].copy_(b_host[(i + 1) % 2], non_blocking=True)
-                        ev_in[(i + 1) % 2].record(cps)
-                xd, st = ctx.solve(gauge, b_dev[i % 2], MASS, op="eo_normal", tol=TOL, maxiter=4000, inner="half")
-                done = torch.cuda.Event()
-                done.record(cur)
-                cps.wait_event(done)
+    def e2e_stream(K):
+        ev_in = [torch.cuda.Event(), torch.cuda.Event()]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(cur)
+        cps.wait_event(e0)
+        with torch.cuda.stream(cps):
+            b_dev[0].copy_(b_host[0], non_blocking=True)
+            ev_in[0].record(cps)
+        last = None
+        for i in range(K):
+            cur.wait_event(ev_in[i % 2])
+            if i + 1 < K:
                 with torch.cuda.stream(cps):
-                    x_host[i % 2].copy_(xd, non_blocking=True)
-                    xd.record_stream(cps)
-                last = st
-            drained = torch.cuda.Event()
-            drained.record(cps)
-            cur.wait_event(drained)
-            e1.record(cur)
-            e1.synchronize()
-            return e0.elapsed_time(e1) / 1e3, last
+                    b_dev[(i + 1) % 2].copy_(b_host[(i + 1) % 2], non_blocking=True)
+                    ev_in[(i + 1) % 2].record(cps)
+            xd, st = ctx.solve(gauge, b_dev[i % 2], MASS, op="eo_normal", tol=TOL, maxiter=4000, inner="half")
+            done = torch.cuda.Event()
+            done.record(cur)
+            cps.wait_event(done)
+            with torch.cuda.stream(cps):
+                x_host[i % 2].copy_(xd, non_blocking=True)
+                xd.record_stream(cps)
+            last = st
+        drained = torch.cuda.Event()
+        drained.record(cps)
+        cur.wait_event(drained)
+        e1.record(cur)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, last
 
-        e2e_stream(2)  # warm-up
-        K = max(3, min(args.steps, 5))
-        t_all, st = e2e_stream(K)
-        _, e2e_value = aggregate_over_ranks(t_all / K, NRHS, dist, dev)
-        nbytes = b_host[0].numel() * b_host[0].element_size()
-        e2e = {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(nbytes),
-               "d2h_bytes_per_step": int(nbytes), "steps": K,
-               "note": "copies of neighbouring steps overlap the solve (copy stream, double buffers)",
-               "all_converged": all(s["status"] == 2 for s in st)}
-        del b_dev, b_host, x_host
+    e2e_stream(2)  # warm-up
+    K = max(3, args.steps)
+    t_all, st = e2e_stream(K)
+    _, e2e_value = aggregate_over_ranks(t_all / K, NRHS, dist, dev)
+    nbytes = b_host[0].numel() * b_host[0].element_size()
+    e2e = {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(nbytes),
+           "d2h_bytes_per_step": int(nbytes), "steps": K,
+           "note": "copies of neighbouring steps overlap the solve (copy stream, double buffers)",
+           "all_converged": all(s["status"] == 2 for s in st)}
+    del b_dev, b_host, x_host
 
     # ---- serving: Poisson stream of propagator requests, continuous batching
     serve = None
@@ -368,23 +375,26 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, SHAPE)), "kappa": KAPPA,
                        "nrhs": NRHS, "tol": TOL, "parallelism": f"replicas x{world} (independent solves)",
                        "l2": "working set > 126 MB L2 (no flush needed)"},
-            "fp64_cg": {"solves_per_s": fp64_sps * world, "iters": it64, "note": "plain FP64 CG, one RHS at a time"},
-            "speedup_vs_fp64": value / (fp64_sps * world),
-            "solve": {"inner": args.inner, "delta": args.delta, "iters_min": min(iters), "iters_max": max(iters),
-                      "max_true_res": res, "all_converged": conv,
-                      "reliable_updates_max": max(s["reliable_updates"] for s in all_stats[-1])},
             "roofline": {"bound": "hbm", "kernel": "hop (FP16 storage, 12-real links, 16 RHS, EO parity)",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": hop_bytes,
                          "ms_per_launch": hop_ms, "traffic": traffic,
-                         **naive_rate(np.prod(SHAPE) // 2, NRHS, 52, 24, hop_ms)},
-            "dslash": dslash_native,
-            "dslash_fp64_reference_layout": dslash,
-            "e2e": e2e,
-            "serve": serve,
+                         **naive_rate(np.prod(SHAPE) // 2, NRHS, 52, 24, hop_ms),
+                         **ref_gflops(DIRAC.flops_per_site_dslash(3) * int(np.prod(SHAPE)) // 2 * NRHS, hop_ms,
+                                      "flops_per_site_dslash x Vh x 16 RHS")},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "e2e": e2e,
+            "serve": serve,
+            # kept last, so that a tail of the line still holds them
+            "dslash": dslash_native,
+            "dslash_fp64_reference_layout": dslash,
+            "solve": {"inner": args.inner, "delta": args.delta, "iters_min": min(iters), "iters_max": max(iters),
+                      "max_true_res": res, "all_converged": conv,
+                      "reliable_updates_max": max(s["reliable_updates"] for s in all_stats[-1])},
+            "fp64_cg": {"solves_per_s": fp64_sps * world, "iters": it64, "note": "plain FP64 CG, one RHS at a time"},
+            "speedup_vs_fp64": value / (fp64_sps * world),
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -426,31 +436,39 @@ def run_serving(args, dev):
 
 
 # --------------------------------------------------------------------------- CPU legs
+# Both CPU legs (the cpu_baseline of our arm and the --impl reference arm) time the
+# same unit: one call of the C restatement's FP64 CG running CPU_ITERS_PER_CALL
+# iterations of M^dag M on the full 24^3x48 system (a quarter of a solve, so
+# per-call set-up is amortised the same way in both), converted to solves/s with
+# the iteration count plain FP64 CG needs to reach 1e-10 on this system.
+CPU_ITERS_PER_CALL = 39
+
+
+def cpu_seconds_per_iter(cw, be, calls: int):
+    """Per-iteration seconds of `calls` timed CG calls (x = 0 start, no early stop)."""
+    out = []
+    for _ in range(calls):
+        t0 = time.perf_counter()
+        cw.cg(be, 0.0, CPU_ITERS_PER_CALL)
+        out.append((time.perf_counter() - t0) / CPU_ITERS_PER_CALL)
+    return out
+
+
 def cpu_baseline(U4, b_full, iters_to_converge: int, seconds: float):
-    """Time FP64 EO CG iterations of the C restatement on all host cores on
-    the full 24^3x48 system for ~`seconds`, and convert to solves/s with the
-    iteration count FP64 CG needs on this system."""
+    """The C restatement on all host cores for about `seconds` (whole calls)."""
     from oracle import cpu as C
     from oracle import wilson as W
 
     C.build()
     cw = C.CpuWilson(U4, SHAPE, BC, MASS)
     be = W.pack(b_full[None], 0)[0]
-    x, k, _ = cw.cg(be, 0.0, 1)  # warm-up (1 iteration)
-    n = 2
-    t0 = time.perf_counter()
-    x, k, _ = cw.cg(be, 0.0, n)
-    t1 = time.perf_counter()
-    per = (t1 - t0) / n
-    n2 = max(1, int(seconds / max(per, 1e-6)) - n)
-    if n2 > 0:
-        t2 = time.perf_counter()
-        cw.cg(be, 0.0, n2)
-        per = (time.perf_counter() - t2) / n2
-        n += n2
+    first = cpu_seconds_per_iter(cw, be, 1)[0]  # warm-up call (thread start, first touch)
+    calls = max(1, int(seconds / max(first * CPU_ITERS_PER_CALL, 1e-6)))
+    per = float(np.mean(cpu_seconds_per_iter(cw, be, calls)))
     return {"value": 1.0 / (per * iters_to_converge), "unit": "solves/s", "cores": C.threads(), "kind": "port",
-            "sample": f"{n} FP64 CG iterations of M^dag M on the full 24^3x48 system, 1 RHS; solves/s = 1/"
-                      f"(s/iter x {iters_to_converge} iters to 1e-10)", "s_per_iter": per}
+            "sample": f"{calls} calls x {CPU_ITERS_PER_CALL} FP64 CG iterations of M^dag M on the full 24^3x48 "
+                      f"system, 1 RHS; solves/s = 1/(s/iter x {iters_to_converge} iters to 1e-10)",
+            "s_per_iter": per}
 
 
 def run_reference(args):
@@ -468,24 +486,17 @@ def run_reference(args):
     C.build()
     cw = C.CpuWilson(U.numpy(), SHAPE, BC, MASS)
     be = cw.normal(W.pack(eta[12:13].numpy(), 0)[0])  # an even RHS of the system; only timing is used
-    per_step = []
-    its = 4
-    for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        cw.cg(be, 0.0, its)
-        dt = (time.perf_counter() - t0) / its
-        if i >= args.warmup:
-            per_step.append(dt)
-    per = float(np.mean(per_step))
+    cpu_seconds_per_iter(cw, be, args.warmup)
+    per = float(np.mean(cpu_seconds_per_iter(cw, be, args.steps)))
     iters = args.ref_iters
     value = 1.0 / (per * iters)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * its * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * CPU_ITERS_PER_CALL * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, SHAPE)), "kappa": KAPPA},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": C.threads(), "kind": "port",
-                             "sample": f"{its} FP64 CG iterations per step on the full system, 1 RHS; solves/s = "
-                                       f"1/(s/iter x {iters} iterations FP64 CG needs to 1e-10)"},
+                             "sample": f"{CPU_ITERS_PER_CALL} FP64 CG iterations per step on the full system, 1 RHS; "
+                                       f"solves/s = 1/(s/iter x {iters} iterations FP64 CG needs to 1e-10)"},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "jaxQFT needs JAX, which is not installable offline; its EO CG is timed via the C restatement"}
     print(json.dumps(line), flush=True)
@@ -584,6 +595,12 @@ def run_profile(args):
     print(json.dumps({"profile": "eo_normal CG iterations", "shape": SHAPE, "nrhs": args.nrhs, "inner": args.inner,
                       "iters": args.profile_iters, "ms_per_iter_wall": (t1 - t0) * 1e3 / args.profile_iters,
                       "hop_us": ms * 1e3, "hop_GBps": by / ms / 1e6}), flush=True)
+
+
+def ref_gflops(flops, ms, how):
+    """GFLOP/s on the reference's own flop count (jaxqft/fermions/wilson.py:349-437)."""
+    return {"ref_flops_per_launch": int(flops), "ref_gflops": float(flops) / (ms * 1e-3) / 1e9,
+            "ref_flops_count": f"WilsonDiracOperator.{how} (nc=3, sparse gamma)"}
 
 
 def naive_rate(sites, nrhs, spinor_bytes, link_bytes, ms):

@@ -177,8 +177,8 @@ wl_status wl_engine_time_update_hop(wl_engine* eng, int reps, double* ms_per_lau
 /* Apply the engine's iterated (sloppy-precision) operator to one
    reference-layout field through slot 0's buffers, for testing the FP16/FP32
    operators against FP64: stage 0 -> K_oe x_e (odd sites of out), 1 -> M x_e,
-   2 -> M^dag M x_e (EO engines; even sites of out), 3 -> D x, 4 -> D^dag D x
-   (full-lattice engines).  Overwrites slot 0's work fields.  Synchronous. */
+   2 -> M^dag M x_e (EO engines; even sites of out), 3 -> D x, 4 -> D^dag D x,
+   5 -> D^dag x (full-lattice engines).  Overwrites slot 0's work fields.  Synchronous. */
 wl_status wl_engine_debug_apply(wl_engine* eng, int stage, double mass, const void* in, void* out);
 /* Number of kernels this library has launched in the process so far
    (graph launches count every kernel node of the graph). */

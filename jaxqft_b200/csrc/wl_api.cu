@@ -22,6 +22,7 @@
 #include "wl_force.cuh"
 #include "wl_gauge.cuh"
 #include "wl_meas.cuh"
+#include "wl_refsite.cuh"
 #include "wl_rowhop.cuh"
 #include "wl_hop_fast.cuh"
 #include "wl_site.cuh"
@@ -570,14 +571,23 @@ static wl_status ensure_tmp(wl_ctx* ctx, size_t bytes) {
   return WL_OK;
 }
 
-// out(target parities) = a*self + b*hop(in); npar = 2 for both parities, else target parity0 only
-static bool row_hop_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("WL_ROW_HOP");
-    return !(e && e[0] == '0');
+// Kernel for the reference-layout hop: 0 = ref_pair_kernel (two threads per
+// site, 256-bit spinor accesses, parity-split SoA links; the default),
+// 1 = row_hop_kernel (TMA row staging), 2 = hop_kernel on the reference layout,
+// 3 = ref_site_kernel (one thread per site).  WL_REF_HOP=pair|row|generic|tps
+// selects one (for comparisons).
+static int ref_hop_kind() {
+  static const int k = [] {
+    const char* e = std::getenv("WL_REF_HOP");
+    if (!e) return 0;
+    if (std::strcmp(e, "row") == 0) return 1;
+    if (std::strcmp(e, "generic") == 0) return 2;
+    if (std::strcmp(e, "tps") == 0) return 3;
+    return 0;
   }();
-  return on;
+  return k;
 }
+static bool row_hop_enabled() { return ref_hop_kind() == 1; }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link needed)
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -642,9 +652,42 @@ static bool row_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const v
   return true;
 }
 
+// Site-parallel reference-layout hop (wl_refsite.cuh); parity < 0 targets every site.
+template <bool DAG>
+static bool site_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const void* self, double a, double b,
+                     int nrhs, int parity) {
+  const Geom& g = ctx->g;
+  const int kind = ref_hop_kind();
+  if ((kind != 0 && kind != 3) || nrhs > 65535) return false;
+  RefSiteArgs A{};
+  A.g = g;
+  A.U = G->d18;
+  A.in = (const double*)in;
+  A.out = (double*)out;
+  A.self = (const double*)self;
+  A.a = a;
+  A.b = b;
+  A.nrhs = nrhs;
+  A.parity = parity;
+  const long long n = (parity < 0 ? g.V : g.Vh) * (kind == 0 ? 2LL : 1LL);  // threads per field
+  const dim3 grid((unsigned)((n + kRefSiteBlock - 1) / kRefSiteBlock), nrhs);
+  const bool w32 = (((uintptr_t)in | (uintptr_t)out | (uintptr_t)self) & 31) == 0;
+  g_launches++;
+  if (kind == 0) {
+    if (w32) ref_pair_kernel<DAG, 4><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
+    else ref_pair_kernel<DAG, 2><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
+  } else {
+    if (w32) ref_site_kernel<DAG, 4><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
+    else ref_site_kernel<DAG, 2><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
+  }
+  return true;
+}
+
+// out(target parities) = a*self + b*hop(in); npar = 2 for both parities, else target parity0 only
 template <bool DAG>
 static void ref_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const void* self, double a, double b,
                     int nrhs, int parity0, int npar) {
+  if (site_hop<DAG>(ctx, G, in, out, self, a, b, nrhs, npar == 2 ? -1 : parity0)) return;
   if (row_hop<DAG>(ctx, G, in, out, self, a, b, nrhs, npar == 2 ? 3 : (1 << parity0))) return;
   RefHopArgs A = ref_args(ctx, G, in, out, self, a, b, nrhs, parity0);
   Tune t;
@@ -1347,8 +1390,9 @@ static void debug_apply_impl(wl_engine* E, int stage, double mass, const void* i
     A.g = g; A.links = L; A.nrhs = 1;
     sf2<S>(E->p, A.src); A.parity0 = 0; sf2<S>(E->y, A.epi.out); sf2<S>(E->p, A.epi.self);
     A.epi.has_self = 1; A.epi.a = mm; A.epi.b = nh;
-    launch_hop<false, IdxCompact>(E->ts, A, 2, st);
-    if (stage >= 4) {
+    if (stage == 5) launch_hop<true, IdxCompact>(E->ts, A, 2, st);  // D^dag x
+    else launch_hop<false, IdxCompact>(E->ts, A, 2, st);            // D x
+    if (stage == 4) {
       HopArgs<LS, SFS, EpiXpay<SFS, false>> B{};
       B.g = g; B.links = L; B.nrhs = 1;
       sf2<S>(E->y, B.src); B.parity0 = 0; sf2<S>(E->xs, B.epi.out); sf2<S>(E->y, B.epi.self);
@@ -1385,7 +1429,7 @@ extern "C" wl_status wl_engine_debug_apply(wl_engine* E, int stage, double mass,
   wl_ctx* ctx = E->ctx;
   WL_CUDA(ctx, cudaSetDevice(ctx->device));
   const bool eo = E->prm.op == WL_SOLVE_EO_NORMAL;
-  if ((eo && (stage < 0 || stage > 2)) || (!eo && stage != 3 && stage != 4))
+  if ((eo && (stage < 0 || stage > 2)) || (!eo && (stage < 3 || stage > 5)))
     WL_FAIL(ctx, WL_ERR_ARG, "stage does not match the engine's operator");
   cudaStream_t st = engine_stream(E);
   switch (E->sprec) {

@@ -1,0 +1,348 @@
+// FP64 Wilson hop on reference-layout fermions, one thread per target site,
+// for the drop-in operators (D, D^dag, K, the masked and Schur forms).
+//
+// Fermions keep the caller's layout: complex128 [rhs][Lx][Ly][Lz][Lt][4][3],
+// 192 contiguous bytes per site.  sm_100 has 256-bit global loads and stores
+// (ld.global.v4.f64 / st.global.v4.f64), so a thread moves its neighbour's
+// spinor as six 32-byte sectors: every sector a warp requests is used whole,
+// and no shared-memory staging or block barrier is needed.  For mu = 3 only the
+// two spins the projector keeps are loaded (three sectors).  Links come from the
+// gauge object's parity-split SoA copy (double2 [p][mu][9][Vh]), so a warp's
+// link load is two contiguous 256-byte runs (the two parities of 16 compact
+// sites) instead of a 144-byte-stride gather.  Neighbour spinors and the second
+// use of every link (forward from x, backward from x + mu) are L2 hits: the
+// reuse distance is at most one x-slice of the lattice (Ly*Lz*Lt sites).
+//
+// Thread mapping: with both parities targeted (D, D^dag, K) thread i of the
+// grid row owns flat site i, so a warp covers 32 consecutive sites; with one
+// target parity p thread i owns compact site i of parity p.
+//
+// Contract = row_hop_kernel: out = a*self + b*acc on the target sites,
+//   acc = sum_mu [(1 + cf g_mu) U_mu(x) psi(x+mu) + (1 + cb g_mu) U_mu^dag(x-mu) psi(x-mu)],
+// cf = -1 (D) or +1 (D^dag), cb = -cf, boundary phase on the forward hop from
+// x_mu = L_mu - 1 and (conjugated) on the backward hop into x_mu = 0.
+#pragma once
+#include "wl_hop.cuh"
+
+namespace wl {
+
+struct RefSiteArgs {
+  Geom g;
+  const double2* U;     // FP64 18-real links [p][mu][9][Vh]
+  const double* in;     // [nrhs][V][24] reals
+  double* out;          // [nrhs][V][24]
+  const double* self;   // [nrhs][V][24] or nullptr
+  double a, b;
+  int nrhs;
+  int parity;           // target parity, or -1 for every site
+};
+
+// 32-byte (W = 4) or 16-byte (W = 2) vector accesses of doubles.  The 32-byte
+// form needs 32-byte aligned addresses; launchers check the field pointers
+// (sites are 192 bytes apart, a multiple of 32).
+template <int W>
+WL_D void ld_vec(const double* p, double* v) {
+  if (W == 4) {
+    asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+                 : "l"(p));
+  } else {
+    const double2 q = __ldg(reinterpret_cast<const double2*>(p));
+    v[0] = q.x;
+    v[1] = q.y;
+  }
+}
+template <int W>
+WL_D void st_vec(double* p, const double* v) {
+  if (W == 4) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3])
+                 : "memory");
+  } else {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  }
+}
+
+// reals [lo, hi) of one site's 24
+template <int W, int LO, int HI>
+WL_D void ld_site_part(const double* site, double (&v)[24]) {
+#pragma unroll
+  for (int k = LO; k < HI; k += W) ld_vec<W>(site + k, v + k);
+}
+
+template <int MU, int C, bool DAGU, int W>
+WL_D void refsite_dir(const double* src, const double2* lk, unsigned vh, bool ph, const Geom& g,
+                      Spinor<double>& acc) {
+  double v[24];
+  // mu = 3 projects onto spins (0, 1) for C > 0 and (2, 3) for C < 0: load only those
+  constexpr int lo = (MU == 3 && C < 0) ? 12 : 0;
+  constexpr int hi = (MU == 3 && C > 0) ? 12 : 24;
+  ld_site_part<W, lo, hi>(src, v);
+  Spinor<double> s;
+#pragma unroll
+  for (int k = 0; k < 12; ++k) s.v[k / 3][k % 3] = (2 * k >= lo && 2 * k < hi) ? cplx<double>{v[2 * k], v[2 * k + 1]}
+                                                                               : cplx<double>{0.0, 0.0};
+  Link<double> u;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const double2 q = ldg(lk + (size_t)k * vh);
+    u.m[k / 3][k % 3] = {q.x, q.y};
+  }
+  Half<double> h, uh;
+  spin_project<MU, C>(s, h);
+  color_mul<DAGU>(u, h, uh);
+  if (ph) phase_mul(uh, g.ph_re[MU], DAGU ? -g.ph_im[MU] : g.ph_im[MU]);
+  spin_accum<MU, C>(acc, uh);
+}
+
+template <int MU, bool DAG, int W>
+WL_D void refsite_mu(const RefSiteArgs& A, const double* base, const Site& s, int parity, Spinor<double>& acc) {
+  constexpr int CF = DAG ? +1 : -1;
+  constexpr int CB = -CF;
+  const Geom& g = A.g;
+  const unsigned vh = (unsigned)g.Vh;
+  {  // forward: U_mu(x) psi(x+mu); the link is stored with the target site's parity
+    const int nb = neighbor(g, s, MU, +1);
+    const int tn = MU == 3 ? (s.x[3] == g.L[3] - 1 ? 0 : s.x[3] + 1) : s.x[3];
+    const double* src = base + (size_t)(2 * nb + (tn & 1)) * 24;
+    const double2* lk = A.U + (size_t)(parity * 4 + MU) * 9 * vh + s.c;
+    refsite_dir<MU, CF, false, W>(src, lk, vh, g.ph_on[MU] && s.x[MU] == g.L[MU] - 1, g, acc);
+  }
+  {  // backward: U_mu(x-mu)^dag psi(x-mu); the link is stored with the other parity
+    const int nb = neighbor(g, s, MU, -1);
+    const int tn = MU == 3 ? (s.x[3] == 0 ? g.L[3] - 1 : s.x[3] - 1) : s.x[3];
+    const double* src = base + (size_t)(2 * nb + (tn & 1)) * 24;
+    const double2* lk = A.U + (size_t)((1 - parity) * 4 + MU) * 9 * vh + nb;
+    refsite_dir<MU, CB, true, W>(src, lk, vh, g.ph_on[MU] && s.x[MU] == 0, g, acc);
+  }
+}
+
+#ifndef WL_REFSITE_MINB
+#define WL_REFSITE_MINB 3  // resident 128-thread blocks per SM the kernel is compiled for
+#endif
+constexpr int kRefSiteBlock = 128;
+
+template <bool DAG, int W>
+__global__ void __launch_bounds__(kRefSiteBlock, WL_REFSITE_MINB) ref_site_kernel(RefSiteArgs A) {
+  const Geom& g = A.g;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  Site s;
+  int parity;
+  if (A.parity < 0) {  // every site: i is the flat index
+    if (i >= g.V) return;
+    const int c = i >> 1;
+    const int row = (int)fdiv(g.fd_lth, (unsigned)c);
+    const int t = i - row * g.L[3];
+    const int r2 = (int)fdiv(g.fd_l2, (unsigned)row);
+    s.c = WL_CHECKED(c, g.Vh);
+    s.row = row;
+    s.x[2] = row - r2 * g.L[2];
+    s.x[0] = (int)fdiv(g.fd_l1, (unsigned)r2);
+    s.x[1] = r2 - s.x[0] * g.L[1];
+    s.x[3] = t;
+    parity = (s.x[0] + s.x[1] + s.x[2] + t) & 1;
+  } else {  // one parity: i is the compact index
+    if (i >= g.Vh) return;
+    parity = A.parity;
+    s = site_from_compact(g, parity, i);
+  }
+  const size_t flat = (size_t)s.row * g.L[3] + s.x[3];
+  const size_t field = (size_t)rhs * g.V * 24;
+  const double* base = A.in + field;
+  Spinor<double> acc;
+  zero(acc);
+  refsite_mu<0, DAG, W>(A, base, s, parity, acc);
+  refsite_mu<1, DAG, W>(A, base, s, parity, acc);
+  refsite_mu<2, DAG, W>(A, base, s, parity, acc);
+  refsite_mu<3, DAG, W>(A, base, s, parity, acc);
+  double o[24];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    o[2 * k] = A.b * acc.v[k / 3][k % 3].re;
+    o[2 * k + 1] = A.b * acc.v[k / 3][k % 3].im;
+  }
+  if (A.self) {
+    double x[24];
+    ld_site_part<W, 0, 24>(A.self + field + flat * 24, x);
+#pragma unroll
+    for (int k = 0; k < 24; ++k) o[k] = fma(A.a, x[k], o[k]);
+  }
+  double* dst = A.out + field + flat * 24;
+#pragma unroll
+  for (int k = 0; k < 24; k += W) st_vec<W>(dst + k, o + k);
+}
+
+// ---------------------------------------------------------------- two threads per site
+// Thread j (j = lane & 1) of a pair forms half-spinor row j of every hop (as
+// hop_pair_kernel does on the internal layout):
+//   mu=0: h = s_j + c s_{3-j}        mu=1: h = s_j + (1-2j) c' s_{3-j}
+//   mu=2: h = s_j + c' s_{2+j}       mu=3: 2 s_j (c = +1) or 2 s_{2+j} (c = -1)
+// with c' = -i c.  In the reference layout spin s is reals [6s, 6s+6): one
+// 32-byte vector plus one 16-byte half.  The pair's 16-byte halves of spins
+// (0, 1) and of spins (2, 3) share a sector and are requested by the same
+// instruction, so a pair requests every sector of a neighbour's spinor exactly
+// once.  Both threads read the same link addresses in the same instruction.
+// Thread j keeps its upper spin A = a_j and partial sums X of a_{3-j} and Y of
+// a_{2+j} (18 doubles instead of 24); at the end two xor-shuffle rounds give
+// thread 0 spins (0, 1) and thread 1 spins (2, 3), and each stores its half of
+// the site with three 32-byte stores.
+
+// spin s (6 reals) of one site: the 32-byte vector and the 16-byte half
+template <int W>
+WL_D void ld_spin(const double* site, int s, double (&v)[6]) {
+  const double* p = site + 6 * s;
+  if (W == 4) {
+    if (s & 1) {  // reals [6s, 6s+2) are the upper half of a 32-byte vector, [6s+2, 6s+6) a whole one
+      const double2 q = __ldg(reinterpret_cast<const double2*>(p));
+      v[0] = q.x;
+      v[1] = q.y;
+      ld_vec<4>(p + 2, v + 2);
+    } else {  // [6s, 6s+4) whole, [6s+4, 6s+6) the lower half of the next
+      ld_vec<4>(p, v);
+      const double2 q = __ldg(reinterpret_cast<const double2*>(p + 4));
+      v[4] = q.x;
+      v[5] = q.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 6; k += 2) ld_vec<2>(p + k, v + k);
+  }
+}
+
+template <int MU, int C, int W>
+WL_D void refpair_project(const double* site, int j, double sg, cplx<double> (&h)[3]) {
+  const int s1 = (MU == 3 && C < 0) ? 2 + j : j;
+  double a[6];
+  ld_spin<W>(site, s1, a);
+  if (MU == 3) {
+#pragma unroll
+    for (int col = 0; col < 3; ++col) h[col] = {2.0 * a[2 * col], 2.0 * a[2 * col + 1]};
+    return;
+  }
+  const int s2 = MU == 2 ? 2 + j : 3 - j;
+  double b[6];
+  ld_spin<W>(site, s2, b);
+#pragma unroll
+  for (int col = 0; col < 3; ++col) {
+    const cplx<double> av{a[2 * col], a[2 * col + 1]}, bv{b[2 * col], b[2 * col + 1]};
+    if (MU == 0) {
+      h[col] = C > 0 ? av + bv : av - bv;
+    } else {
+      const cplx<double> w = C > 0 ? mul_mi(bv) : mul_i(bv);  // -i C b
+      if (MU == 1) h[col] = {fma(sg, w.re, av.re), fma(sg, w.im, av.im)};
+      else h[col] = av + w;
+    }
+  }
+}
+
+template <int MU, bool DAG, int W>
+WL_D void refpair_mu(const RefSiteArgs& A, const double* base, const Site& s, int parity, int j, double sg,
+                     cplx<double> (&Ac)[3], cplx<double> (&Xc)[3], cplx<double> (&Yc)[3]) {
+  constexpr int CF = DAG ? +1 : -1;
+  constexpr int CB = -CF;
+  const Geom& g = A.g;
+  const unsigned vh = (unsigned)g.Vh;
+#pragma unroll
+  for (int dir = 0; dir < 2; ++dir) {
+    const int nb = neighbor(g, s, MU, dir == 0 ? +1 : -1);
+    int tn = s.x[3];
+    if (MU == 3) tn = dir == 0 ? (tn == g.L[3] - 1 ? 0 : tn + 1) : (tn == 0 ? g.L[3] - 1 : tn - 1);
+    const double* src = base + (size_t)(2 * nb + (tn & 1)) * 24;
+    const double2* lk = dir == 0 ? A.U + (size_t)(parity * 4 + MU) * 9 * vh + s.c
+                                 : A.U + (size_t)((1 - parity) * 4 + MU) * 9 * vh + nb;
+    Link<double> u;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const double2 q = ldg(lk + (size_t)k * vh);
+      u.m[k / 3][k % 3] = {q.x, q.y};
+    }
+    cplx<double> h[3];
+    if (dir == 0) {
+      refpair_project<MU, CF, W>(src, j, sg, h);
+      pair_hop<MU, CF, false>(u, h, g.ph_on[MU] && s.x[MU] == g.L[MU] - 1, g, sg, Ac, Xc, Yc);
+    } else {
+      refpair_project<MU, CB, W>(src, j, sg, h);
+      pair_hop<MU, CB, true>(u, h, g.ph_on[MU] && s.x[MU] == 0, g, sg, Ac, Xc, Yc);
+    }
+  }
+}
+
+#ifndef WL_REFPAIR_MINB
+#define WL_REFPAIR_MINB 4  // resident 128-thread blocks per SM the pair kernel is compiled for
+#endif
+
+template <bool DAG, int W>
+__global__ void __launch_bounds__(kRefSiteBlock, WL_REFPAIR_MINB) ref_pair_kernel(RefSiteArgs A) {
+  const Geom& g = A.g;
+  const int i = blockIdx.x * (blockDim.x >> 1) + (threadIdx.x >> 1);
+  const int j = threadIdx.x & 1;
+  const double sg = 1.0 - 2.0 * j;
+  const int rhs = blockIdx.y;
+  const bool act = i < (A.parity < 0 ? g.V : g.Vh);
+  Site s{};
+  int parity = 0;
+  cplx<double> Ac[3], Xc[3], Yc[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) Ac[a] = Xc[a] = Yc[a] = {0.0, 0.0};
+  const size_t field = (size_t)rhs * g.V * 24;
+  if (act) {
+    if (A.parity < 0) {  // every site: i is the flat index
+      const int c = i >> 1;
+      const int row = (int)fdiv(g.fd_lth, (unsigned)c);
+      const int t = i - row * g.L[3];
+      const int r2 = (int)fdiv(g.fd_l2, (unsigned)row);
+      s.c = WL_CHECKED(c, g.Vh);
+      s.row = row;
+      s.x[2] = row - r2 * g.L[2];
+      s.x[0] = (int)fdiv(g.fd_l1, (unsigned)r2);
+      s.x[1] = r2 - s.x[0] * g.L[1];
+      s.x[3] = t;
+      parity = (s.x[0] + s.x[1] + s.x[2] + t) & 1;
+    } else {  // one parity: i is the compact index
+      parity = A.parity;
+      s = site_from_compact(g, parity, i);
+    }
+    const double* base = A.in + field;
+    refpair_mu<0, DAG, W>(A, base, s, parity, j, sg, Ac, Xc, Yc);
+    refpair_mu<1, DAG, W>(A, base, s, parity, j, sg, Ac, Xc, Yc);
+    refpair_mu<2, DAG, W>(A, base, s, parity, j, sg, Ac, Xc, Yc);
+    refpair_mu<3, DAG, W>(A, base, s, parity, j, sg, Ac, Xc, Yc);
+  }
+  // a0 = A_0, a1 = A_1, a2 = Y_0 + X_1, a3 = X_0 + Y_1 (subscript = thread of the pair).
+  // Round 1: thread 0 sends X_0 and receives A_1; round 2: thread 0 sends Y_0.
+  cplx<double> lo[3], hi[3];  // thread 0: spins 0, 1; thread 1: spins 2, 3
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const cplx<double> r1 = shfl_pair(j == 0 ? Xc[a] : Ac[a]);
+    const cplx<double> r2 = shfl_pair(Yc[a]);
+    if (j == 0) {
+      lo[a] = Ac[a];
+      hi[a] = r1;
+    } else {
+      lo[a] = r2 + Xc[a];  // a2 = Y_0 + X_1
+      hi[a] = r1 + Yc[a];  // a3 = X_0 + Y_1
+    }
+  }
+  if (!act) return;
+  const size_t flat = (size_t)s.row * g.L[3] + s.x[3];
+  double o[12];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    o[2 * a] = A.b * lo[a].re;
+    o[2 * a + 1] = A.b * lo[a].im;
+    o[6 + 2 * a] = A.b * hi[a].re;
+    o[6 + 2 * a + 1] = A.b * hi[a].im;
+  }
+  const size_t off = field + flat * 24 + 12 * j;  // this thread's two spins
+  if (A.self) {
+    double x[12];
+#pragma unroll
+    for (int k = 0; k < 12; k += W) ld_vec<W>(A.self + off + k, x + k);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) o[k] = fma(A.a, x[k], o[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < 12; k += W) st_vec<W>(A.out + off + k, o + k);
+}
+
+}  // namespace wl

@@ -444,7 +444,7 @@ class Engine:
 
     def debug_apply(self, stage: int, mass: float, x):
         """The engine's iterated-precision operator applied to one field (see
-        wl_engine_debug_apply): 0 K_oe, 1 M, 2 M^dag M (EO); 3 D, 4 D^dag D (full)."""
+        wl_engine_debug_apply): 0 K_oe, 1 M, 2 M^dag M (EO); 3 D, 4 D^dag D, 5 D^dag (full)."""
         import torch
 
         x = _c128(x, self.ctx.device)

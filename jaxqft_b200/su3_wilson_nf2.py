@@ -26,6 +26,7 @@ from . import lib as L
 from .gamma import build_euclidean_gamma
 from .hamiltonian import HamiltonianModel
 from .su3_ym import SU3YangMills, project_su3_algebra
+from .wilson import WilsonDiracOperator
 
 
 def _vdot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
@@ -337,6 +338,9 @@ class SU3WilsonNf2(SU3YangMills):
         self._m0 = float(self.mass + self.wilson_r * self.Nd)
         self.gamma = build_euclidean_gamma(4, dtype=torch.complex128, device=self.device)
         self.Ns = 4
+        # the reference keeps its WilsonDiracOperator as `dirac`; callers read its flop counter
+        self.dirac = WilsonDiracOperator(ndim=4, mass=float(self.mass), wilson_r=float(self.wilson_r),
+                                         dtype=self.dtype, gamma=self.gamma)
         self.ctx = L.WilsonContext(self.lattice_shape, bc=self._bc_phases, device=self.device)
         even, odd, _ = self.ctx.eo_maps()
         self._cb_even_idx = torch.from_numpy(even.astype(np.int64)).to(self.device)

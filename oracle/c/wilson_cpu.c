@@ -192,6 +192,12 @@ static void hop(const wcpu* w, int target, int sign, const cplx* in, cplx* out) 
   par_for((size_t)w->Vh, hop_range, &a);
 }
 
+/* out = K in on compact fields: target-parity sites of -1/2 sum_mu [...] above
+   (sign -1: the hop of D, +1: of D^dag).  Exported for full-size operator checks. */
+void wcpu_hop(const wcpu* w, int target, int sign, const void* in, void* out) {
+  hop(w, target, sign, (const cplx*)in, (cplx*)out);
+}
+
 /* vector kernels */
 typedef struct {
   int kind;

@@ -36,6 +36,7 @@ def lib():
         L.wcpu_create.argtypes = [vp, vp, vp, vp, d]
         L.wcpu_destroy.argtypes = [vp]
         L.wcpu_normal.argtypes = [vp, vp, vp]
+        L.wcpu_hop.argtypes = [vp, i, i, vp, vp]
         L.wcpu_cg.restype = i
         L.wcpu_cg.argtypes = [vp, vp, vp, d, i, ctypes.POINTER(d)]
         L.wcpu_threads.restype = i
@@ -56,12 +57,33 @@ class CpuWilson:
         self.h = lib().wcpu_create(dims.ctypes.data, self._re.ctypes.data, self._im.ctypes.data, self.U.ctypes.data,
                                    float(mass))
         self.vh = int(np.prod(self.shape)) // 2
+        self.m0 = float(mass) + 4.0
 
     def normal(self, x):
         x = np.ascontiguousarray(x, dtype=np.complex128)
         out = np.empty_like(x)
         lib().wcpu_normal(self.h, x.ctypes.data, out.ctypes.data)
         return out
+
+    def hop(self, target, sign, x):
+        """K x on compact fields: the target-parity sites of -1/2 sum_mu of the
+        hops of D (sign -1) or D^dag (sign +1) from the other parity's x."""
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        out = np.empty_like(x)
+        lib().wcpu_hop(self.h, int(target), int(sign), x.ctypes.data, out.ctypes.data)
+        return out
+
+    def apply_D(self, psi, dag=False):
+        """D (or D^dag) on one reference-layout field [*shape, 4, 3], from the
+        compact hops: (D x)_p = m0 x_p + K_{p,1-p} x_{1-p}."""
+        from oracle import wilson as W
+
+        sign = 1 if dag else -1
+        m0 = float(self.m0)
+        xe, xo = W.pack(psi[None], 0)[0], W.pack(psi[None], 1)[0]
+        out_e = m0 * xe + self.hop(0, sign, xo)
+        out_o = m0 * xo + self.hop(1, sign, xe)
+        return W.unpack(out_e[None], self.shape, 0)[0] + W.unpack(out_o[None], self.shape, 1)[0]
 
     def cg(self, b, tol, maxiter):
         b = np.ascontiguousarray(b, dtype=np.complex128)

@@ -3,8 +3,11 @@ oracle, on Gaussian and on point-source fields (the latter have most sites
 exactly zero, the hard case for per-site FP16 norms).
 
 Tolerances (relative, Frobenius): FP64 1e-13; FP32 storage + 12-real links
-2e-6; FP16 storage (per-site norm) + 12-real FP16 links with FP32 arithmetic
-4e-3 per application of M^dag M.
+1e-6 for D and D^dag applied to a spinor (the FP32 bound the port is held
+to) and 2e-6 for the composite operators K, M, M^dag M and D^dag D, whose
+cancellations (M = 1 - K K / m0^2 near the critical kappa) amplify the FP32
+rounding of the intermediate field; FP16 storage (per-site norm) + 12-real
+FP16 links with FP32 arithmetic 4e-3 per application of M^dag M.
 """
 
 import numpy as np
@@ -21,6 +24,7 @@ if not torch.cuda.is_available():  # pragma: no cover
 from jaxqft_b200.lib import Engine, WilsonContext  # noqa: E402
 
 TOLS = {"double": 1e-13, "single": 2e-6, "half": 4e-3}
+TOLS_D = {"double": 1e-13, "single": 1e-6, "half": 4e-3}  # D and D^dag applied to a spinor
 
 
 def _fields(shape, seed):
@@ -67,7 +71,11 @@ def test_full_sloppy_operators(setup, inner):
     eng = Engine(ctx, gauge, 1, op="normal", inner=inner)
     for src, x in _fields(shape, 2).items():
         out = eng.debug_apply(3, m, torch.from_numpy(x)).cpu().numpy()
-        assert rel(out, W.apply_D(U, x[None], m, bc)[0]) < TOLS[inner], (inner, src)
+        err = rel(out, W.apply_D(U, x[None], m, bc)[0])
+        assert err < TOLS_D[inner], (inner, src, "D", err)
+        out = eng.debug_apply(5, m, torch.from_numpy(x)).cpu().numpy()
+        err = rel(out, W.apply_Ddag(U, x[None], m, bc)[0])
+        assert err < TOLS_D[inner], (inner, src, "Ddag", err)
         out = eng.debug_apply(4, m, torch.from_numpy(x)).cpu().numpy()
         assert rel(out, W.apply_normal(U, x[None], m, bc)[0]) < TOLS[inner], (inner, src)
     eng.close()
@@ -119,3 +127,27 @@ def test_point_source_long_lattice_half():
         s = W.schur_even(U, xn[r][None], m, bc, normalized=True)
         Ax = W.schur_even(U, s, m, bc, normalized=True, dag=True)[0]
         assert np.linalg.norm(bn[r] - Ax) / np.linalg.norm(bn[r]) <= 1e-10
+
+
+@pytest.mark.parametrize("kappa", [0.12, 0.135])
+@pytest.mark.parametrize("src", ["gauss", "point"])
+def test_fp32_D_within_1e6(setup, kappa, src):
+    """D and D^dag in FP32 (FP32 storage, 12-real FP32 links, FP32 arithmetic)
+    against the FP64 oracle at 1e-6 relative, at both masses of the measured
+    configurations and on a complex boundary phase as well as the antiperiodic one."""
+    shape, U, bc, ctx, gauge = setup
+    m = W.kappa_to_mass(kappa)
+    x = _fields(shape, 3)[src]
+    for c, g, b in ((ctx, gauge, bc), *_phase_ctx(shape, U)):
+        eng = Engine(c, g, 1, op="normal", inner="single")
+        d = eng.debug_apply(3, m, torch.from_numpy(x)).cpu().numpy()
+        dd = eng.debug_apply(5, m, torch.from_numpy(x)).cpu().numpy()
+        eng.close()
+        assert rel(d, W.apply_D(U, x[None], m, b)[0]) < 1e-6, (kappa, src, b)
+        assert rel(dd, W.apply_Ddag(U, x[None], m, b)[0]) < 1e-6, (kappa, src, b)
+
+
+def _phase_ctx(shape, U):
+    bc = (1, 1, complex(np.cos(np.pi / 3), np.sin(np.pi / 3)), -1)
+    ctx = WilsonContext(shape, bc=bc)
+    return [(ctx, ctx.gauge(torch.from_numpy(U[0])), bc)]
