@@ -406,33 +406,26 @@ SERVE_VOLUMES = [(8, 8, 8, 8), (12, 12, 12, 24), (16, 16, 16, 32), (24, 24, 24, 
 
 
 def run_serving(args, dev):
-    """Serving workload: Poisson arrivals (mean 50/s) over `serve_seconds`,
-    volume uniform over {8^4, 12^3x24, 16^3x32, 24^3x48}, kappa uniform in
-    [0.120, 0.135], 1-12 point or Gaussian RHS each, on 4 resident gauge fields
-    per volume (exp(i*0.2*H), seeds 0-3), admission by HBM budget, true residual
-    1e-10.  Latency includes queueing (arrival to last RHS converged)."""
-    from jaxqft_b200.serving import PropagatorServer, Request, poisson_requests, summarize
+    """Serving workload: Poisson arrivals over `serve_seconds` at the configured
+    mean rate (50/s), volume uniform over {8^4, 12^3x24, 16^3x32, 24^3x48}, kappa
+    uniform in [0.120, 0.135], 1-12 point or Gaussian RHS each, on 4 resident
+    gauge fields per volume (exp(i*0.2*H), seeds 0-3), admission by HBM budget,
+    true residual 1e-10; then the same for `serve_seconds2` at `serve_rate2`, a
+    rate one B200 sustains (queue empty when arrivals stop).  Latency includes
+    queueing (arrival to last RHS converged); the queue length is sampled."""
+    from jaxqft_b200.serving import PropagatorServer, serve_once, warm_server
 
     server = PropagatorServer(SERVE_VOLUMES, gauge_seeds=(0, 1, 2, 3), nslots=16, inner="half", tol=TOL,
                               device=dev)
-    # server start-up: one 1-RHS request per (volume, gauge field) pair, so every engine is
-    # allocated, tuned and graph-captured before the timed request stream, as a server does
-    # when it starts (the timed stream itself starts from an idle server)
-    warm = [Request(rid=-1 - i, volume=tuple(v), gauge=g, kappa=0.125, nrhs=1, kind="gaussian", t_arrive=0.0,
-                    seed=99 + i)
-            for i, (v, g) in enumerate((v, g) for v in SERVE_VOLUMES for g in (0, 1, 2, 3))]
-    server.run(warm)
-    server.done = []
-    reqs = poisson_requests(args.serve_rate, args.serve_seconds, SERVE_VOLUMES, seed=1)
-    t0 = time.perf_counter()
-    done = server.run(reqs)
-    wall = time.perf_counter() - t0
-    s = summarize(done, wall)
-    s.update({"rate_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,
-              "volumes": ["x".join(map(str, v)) for v in SERVE_VOLUMES], "gauge_fields_per_volume": 4,
-              "hbm_budget_GB": server.hbm_budget / 1e9, "peak_engine_GB": server.peak_engine_bytes / 1e9})
+    warm_server(server)  # every engine allocated, tuned and graph-captured before the timed streams
+    out = serve_once(server, args.serve_rate, args.serve_seconds)
+    out.update({"volumes": ["x".join(map(str, v)) for v in SERVE_VOLUMES], "gauge_fields_per_volume": 4,
+                "hbm_budget_GB": server.hbm_budget / 1e9, "peak_engine_GB": server.peak_engine_bytes / 1e9})
+    if args.serve_seconds2 > 0:
+        out["sustained"] = serve_once(server, args.serve_rate2, args.serve_seconds2, seed=2)
+        out["sustained"].pop("per_volume", None)
     server.close()
-    return s
+    return out
 
 
 # --------------------------------------------------------------------------- CPU legs
@@ -623,6 +616,10 @@ def main():
     ap.add_argument("--delta", type=float, default=0.1, help="reliable-update threshold of the mixed solver")
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="serving leg: seconds of Poisson arrivals (0: off)")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="serving leg: mean requests per second")
+    ap.add_argument("--serve-seconds2", type=float, default=10.0,
+                    help="serving leg: seconds of arrivals at --serve-rate2 (0: off)")
+    ap.add_argument("--serve-rate2", type=float, default=12.0,
+                    help="serving leg: a mean rate one B200 sustains without queue growth")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--fp64-all", action="store_true", help="time plain FP64 CG on all 16 RHS (default 4)")
     ap.add_argument("--profile-iters", type=int, default=0,

@@ -158,6 +158,14 @@ wl_status wl_engine_admit(wl_engine* eng, const int* slots, int n, const void* b
 wl_status wl_engine_step(wl_engine* eng, int iters);
 /* Synchronise and report per-slot status (0 idle, 1 running, 2..5 stopped). */
 wl_status wl_engine_poll(wl_engine* eng, int* status, int* n_active);
+/* Non-blocking form of wl_engine_poll, for a host loop that drives many
+   engines (no counterpart in the reference, whose solves are synchronous):
+   wl_engine_poll_async queues the status copies on the engine stream behind the
+   work queued so far and returns at once; wl_engine_poll_ready never blocks and
+   returns 1 (status / n_active filled, as wl_engine_poll would), 0 while that
+   work is still running, -1 with no poll queued, -2 on a CUDA error. */
+wl_status wl_engine_poll_async(wl_engine* eng);
+int wl_engine_poll_ready(wl_engine* eng, int* status, int* n_active);
 /* Copy the solution of slot `slot` into x (reference layout) and free the slot. */
 wl_status wl_engine_retire(wl_engine* eng, int slot, void* x, wl_solve_stats* stats);
 /* Size in bytes of the engine's device allocations (for HBM admission). */
@@ -207,6 +215,34 @@ int64_t wl_bounds_errors(long long* first_bad);
    on the GPU (different streams or contexts of one device) race. */
 wl_status wl_apply_schur_normal_noalloc(wl_ctx* ctx, wl_gauge* gauge, double mass, unsigned flags,
                                         const void* in, void* out, int nrhs);
+
+/* Field inner products and combinations ----------------------------------- */
+/* For the chronological initial-guess predictors (su3_wilson_nf2.py:85-194),
+   on complex128 device vectors of `len` elements.  `a`, `b`, `x` are HOST
+   arrays of device pointers.
+   wl_field_dots: out[2k], out[2k+1] = Re, Im of <a_k, b_k> = sum conj(a_k) b_k
+   for k < npairs <= 64 (host array; deterministic order of summation;
+   synchronises the context stream).
+   wl_field_combine: out = sum_k (coef[2k] + i coef[2k+1]) x_k, k < n <= 32;
+   out may be one of the x_k.  Asynchronous on the context stream. */
+wl_status wl_field_dots(wl_ctx* ctx, int npairs, const void* const* a, const void* const* b, int64_t len,
+                        double* out);
+wl_status wl_field_combine(wl_ctx* ctx, int n, const void* const* x, const double* coef, int64_t len, void* out);
+
+/* Random fields ----------------------------------------------------------- */
+/* Gaussian fields from a counter-based generator (Philox4x32-10 with key =
+   seed; every value is a function of (seed, stream, position), so a given
+   (seed, stream) always yields the same field).  Asynchronous on the context
+   stream.  Replace the jax.random draws of random_fermion
+   (jaxqft/models/su3_wilson_nf2.py:1169-1175) and of _sample_algebra /
+   refresh_p (jaxqft/models/su3_ym.py:238-244, 339-347); the streams are not
+   jax's threefry streams.
+   wl_random_spinor: out [n][Lx][Ly][Lz][Lt][4][3] complex128, each component
+   (g0 + i g1)/sqrt(2) with g0, g1 standard normal (E|z|^2 = 1).
+   wl_random_algebra: P [batch][4][Lx][Ly][Lz][Lt][3][3] complex128 (BMXYIJ),
+   P = TA(scale (G1 + i G2)), TA(X) = (X - X^dag)/2 - Tr(X - X^dag)/6. */
+wl_status wl_random_spinor(wl_ctx* ctx, uint64_t seed, uint64_t stream, int n, void* out);
+wl_status wl_random_algebra(wl_ctx* ctx, uint64_t seed, uint64_t stream, int batch, double scale, void* P);
 
 /* Pseudofermion force ----------------------------------------------------- */
 /* F = pseudofermion_force_from_solution(U, X, Y) (su3_wilson_nf2.py:1556-1576):

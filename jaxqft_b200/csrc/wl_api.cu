@@ -23,6 +23,8 @@
 #include "wl_gauge.cuh"
 #include "wl_meas.cuh"
 #include "wl_refsite.cuh"
+#include "wl_rng.cuh"
+#include "wl_blas.cuh"
 #include "wl_rowhop.cuh"
 #include "wl_hop_fast.cuh"
 #include "wl_site.cuh"
@@ -772,6 +774,89 @@ extern "C" wl_status wl_apply(wl_ctx* ctx, wl_gauge* G, int op, double mass, uns
   return check_launch(ctx, "wl_apply");
 }
 
+// ============================================================== field inner products / combinations
+static wl_status ensure_red(wl_ctx* ctx, size_t bytes);
+
+extern "C" wl_status wl_field_dots(wl_ctx* ctx, int npairs, const void* const* a, const void* const* b, int64_t len,
+                                   double* out) {
+  NvtxRange nvtx_range("wl_field_dots");
+  if (!ctx || !a || !b || !out) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
+  if (npairs <= 0 || npairs > kMaxFieldPairs) WL_FAIL(ctx, WL_ERR_ARG, "npairs must be in 1..64");
+  if (len <= 0) WL_FAIL(ctx, WL_ERR_ARG, "len must be positive");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  DotsArgs A{};
+  for (int k = 0; k < npairs; ++k) {
+    if (!a[k] || !b[k]) WL_FAIL(ctx, WL_ERR_ARG, "null field pointer");
+    A.a[k] = (const double2*)a[k];
+    A.b[k] = (const double2*)b[k];
+  }
+  A.len = len;
+  const int nblk = (int)std::min<long long>((len + kBlasThreads - 1) / kBlasThreads, 4LL * ctx->sm_count);
+  wl_status s = ensure_red(ctx, sizeof(double2) * ((size_t)npairs * nblk + npairs));
+  if (s != WL_OK) return s;
+  A.partials = (double2*)ctx->red;
+  A.result = A.partials + (size_t)npairs * nblk;
+  g_launches += 2;
+  field_dots_kernel<<<dim3(nblk, npairs), kBlasThreads, 0, ctx->stream>>>(A);
+  field_dots_finalize_kernel<<<npairs, kBlasThreads, 0, ctx->stream>>>(A, nblk);
+  WL_CUDA(ctx, cudaMemcpyAsync(out, A.result, sizeof(double2) * npairs, cudaMemcpyDeviceToHost, ctx->stream));
+  WL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return check_launch(ctx, "field_dots_kernel");
+}
+
+extern "C" wl_status wl_field_combine(wl_ctx* ctx, int n, const void* const* x, const double* coef, int64_t len,
+                                      void* out) {
+  NvtxRange nvtx_range("wl_field_combine");
+  if (!ctx || !x || !coef || !out) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
+  if (n <= 0 || n > kMaxCombine) WL_FAIL(ctx, WL_ERR_ARG, "n must be in 1..32");
+  if (len <= 0) WL_FAIL(ctx, WL_ERR_ARG, "len must be positive");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  CombineArgs A{};
+  for (int k = 0; k < n; ++k) {
+    if (!x[k]) WL_FAIL(ctx, WL_ERR_ARG, "null field pointer");
+    A.x[k] = (const double2*)x[k];
+    A.c[k] = make_double2(coef[2 * k], coef[2 * k + 1]);
+  }
+  A.n = n;
+  A.len = len;
+  A.out = (double2*)out;
+  const int nblk = (int)std::min<long long>((len + kBlasThreads - 1) / kBlasThreads, 8LL * ctx->sm_count);
+  g_launches++;
+  field_combine_kernel<<<nblk, kBlasThreads, 0, ctx->stream>>>(A);
+  return check_launch(ctx, "field_combine_kernel");
+}
+
+// ============================================================== random fields
+static wl_status launch_rng(wl_ctx* ctx, bool spinor, uint64_t seed, uint64_t stream, int nfield, double scale,
+                            void* out) {
+  if (!ctx || !out) WL_FAIL(ctx, WL_ERR_ARG, "null argument");
+  if (nfield <= 0 || nfield > 65535) WL_FAIL(ctx, WL_ERR_ARG, "field count out of range");
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  RngArgs A{};
+  A.seed = seed;
+  A.stream = stream;
+  A.n_elem = spinor ? (long long)ctx->g.V : 4LL * ctx->g.V;
+  A.nfield = nfield;
+  A.scale = scale;
+  A.out = (double2*)out;
+  const dim3 grid((unsigned)((A.n_elem + 255) / 256), (unsigned)nfield);
+  g_launches++;
+  if (spinor) rng_spinor_kernel<<<grid, 256, 0, ctx->stream>>>(A);
+  else rng_algebra_kernel<<<grid, 256, 0, ctx->stream>>>(A);
+  return check_launch(ctx, spinor ? "rng_spinor_kernel" : "rng_algebra_kernel");
+}
+
+extern "C" wl_status wl_random_spinor(wl_ctx* ctx, uint64_t seed, uint64_t stream, int n, void* out) {
+  NvtxRange nvtx_range("wl_random_spinor");
+  return launch_rng(ctx, true, seed, stream, n, 1.0, out);
+}
+
+extern "C" wl_status wl_random_algebra(wl_ctx* ctx, uint64_t seed, uint64_t stream, int batch, double scale,
+                                       void* P) {
+  NvtxRange nvtx_range("wl_random_algebra");
+  return launch_rng(ctx, false, seed, stream, batch, scale, P);
+}
+
 // ============================================================== force
 extern "C" wl_status wl_pf_force(wl_ctx* ctx, wl_gauge* G, const void* X, const void* Y, double coef, int accumulate,
                                  void* F) {
@@ -945,6 +1030,8 @@ struct wl_engine {
   std::vector<double> h_tol2, h_one, h_neg_half, h_half_alpha, h_m0;
   std::vector<int> h_maxiter, h_admit;
   int* h_pinned = nullptr;
+  cudaEvent_t poll_ev = nullptr;  // recorded after the copies of wl_engine_poll_async
+  bool poll_pending = false;
   // reductions
   double* partials = nullptr;
   unsigned* counters = nullptr;
@@ -1644,6 +1731,7 @@ extern "C" void wl_engine_destroy(wl_engine* E) {
   cudaFree(E->counters);
   cudaFree(E->ru_iters);
   if (E->h_pinned) cudaFreeHost(E->h_pinned);
+  if (E->poll_ev) cudaEventDestroy(E->poll_ev);
   if (st) cudaStreamDestroy(st);
   {
     std::lock_guard<std::mutex> lk(g_es_mu);
@@ -1727,6 +1815,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   if (e == cudaSuccess) e = cudaMalloc(&E->counters, sizeof(unsigned) * (n + 1));
   if (e == cudaSuccess) e = cudaMallocHost(&E->h_pinned, sizeof(int) * (3 * n + 2));
   if (e == cudaSuccess) e = cudaMalloc(&E->ru_iters, sizeof(int));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->poll_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     ctx->err = std::string("engine allocation: ") + cudaGetErrorString(e);
     wl_engine_destroy(E);
@@ -1996,15 +2085,20 @@ extern "C" wl_status wl_engine_time_update_hop(wl_engine* E, int reps, double* m
   return WL_OK;
 }
 
-extern "C" wl_status wl_engine_poll(wl_engine* E, int* status, int* n_active) {
-  if (!E) WL_FAIL(nullptr, WL_ERR_ARG, "null engine");
+// Copies of the active count, the per-slot status and the conditional-body counter into the
+// engine's pinned host buffer, queued on the engine stream.
+static wl_status enqueue_poll_copies(wl_engine* E, cudaStream_t st) {
   wl_ctx* ctx = E->ctx;
-  cudaStream_t st = engine_stream(E);
   const int n = E->n;
   WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned, E->n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
-  if (status) WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned + 1, E->status, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned + 1, E->status, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
   WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned + 1 + n, E->ru_iters, sizeof(int), cudaMemcpyDeviceToHost, st));
-  WL_CUDA(ctx, cudaStreamSynchronize(st));
+  return WL_OK;
+}
+
+// Read the pinned buffer once its copies have completed.
+static void read_poll_copies(wl_engine* E, int* status, int* n_active) {
+  const int n = E->n;
   {  // kernels that ran inside the graph's conditional reliable-update body
     const long long seen = E->h_pinned[1 + n];
     g_launches += (seen - E->ru_iters_seen) * E->ru_body_kernels;
@@ -2012,7 +2106,42 @@ extern "C" wl_status wl_engine_poll(wl_engine* E, int* status, int* n_active) {
   }
   if (n_active) *n_active = E->h_pinned[0];
   if (status) std::memcpy(status, E->h_pinned + 1, sizeof(int) * n);
+}
+
+extern "C" wl_status wl_engine_poll(wl_engine* E, int* status, int* n_active) {
+  if (!E) WL_FAIL(nullptr, WL_ERR_ARG, "null engine");
+  wl_ctx* ctx = E->ctx;
+  cudaStream_t st = engine_stream(E);
+  wl_status s = enqueue_poll_copies(E, st);
+  if (s != WL_OK) return s;
+  WL_CUDA(ctx, cudaStreamSynchronize(st));
+  E->poll_pending = false;
+  read_poll_copies(E, status, n_active);
   return WL_OK;
+}
+
+extern "C" wl_status wl_engine_poll_async(wl_engine* E) {
+  if (!E) WL_FAIL(nullptr, WL_ERR_ARG, "null engine");
+  wl_ctx* ctx = E->ctx;
+  cudaStream_t st = engine_stream(E);
+  wl_status s = enqueue_poll_copies(E, st);
+  if (s != WL_OK) return s;
+  WL_CUDA(ctx, cudaEventRecord(E->poll_ev, st));
+  E->poll_pending = true;
+  return WL_OK;
+}
+
+extern "C" int wl_engine_poll_ready(wl_engine* E, int* status, int* n_active) {
+  if (!E || !E->poll_pending) return -1;
+  const cudaError_t q = cudaEventQuery(E->poll_ev);
+  if (q == cudaErrorNotReady) return 0;
+  if (q != cudaSuccess) {
+    E->ctx->err = std::string("wl_engine_poll_ready: ") + cudaGetErrorString(q);
+    return -2;
+  }
+  E->poll_pending = false;
+  read_poll_copies(E, status, n_active);
+  return 1;
 }
 
 static wl_status engine_stats(wl_engine* E, wl_solve_stats* stats, int first, int count) {

@@ -39,10 +39,11 @@ EXPORTS = (
     "wl_version", "wl_ctx_create", "wl_ctx_destroy", "wl_last_error", "wl_ctx_set_stream",
     "wl_ctx_synchronize", "wl_eo_maps", "wl_gauge_create", "wl_gauge_update", "wl_gauge_unitarity",
     "wl_gauge_destroy", "wl_apply", "wl_solve", "wl_engine_create", "wl_engine_destroy", "wl_engine_admit",
-    "wl_engine_step", "wl_engine_poll", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
+    "wl_engine_step", "wl_engine_poll", "wl_engine_poll_async", "wl_engine_poll_ready", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
     "wl_engine_stream", "wl_engine_time_hop", "wl_engine_time_update_hop", "wl_kernel_launches", "wl_engine_debug_apply",
     "wl_apply_schur_normal_noalloc", "wl_gauge_force", "wl_gauge_evolve", "wl_gauge_plaquette_sum",
-    "wl_momentum_kinetic", "wl_pion_correlator", "wl_bounds_errors",
+    "wl_momentum_kinetic", "wl_pion_correlator", "wl_bounds_errors", "wl_random_spinor", "wl_random_algebra",
+    "wl_field_dots", "wl_field_combine",
 )
 
 
@@ -101,6 +102,8 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wl_engine_admit": (i, [vp, pi, i, vp, pd, pd, pi]),
         "wl_engine_step": (i, [vp, i]),
         "wl_engine_poll": (i, [vp, pi, pi]),
+        "wl_engine_poll_async": (i, [vp]),
+        "wl_engine_poll_ready": (i, [vp, pi, pi]),
         "wl_engine_retire": (i, [vp, i, vp, ctypes.POINTER(WLSolveStats)]),
         "wl_engine_bytes": (ctypes.c_int64, [vp, i, i, i]),
         "wl_pf_force": (i, [vp, vp, vp, vp, d, i, vp]),
@@ -116,6 +119,10 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wl_gauge_plaquette_sum": (i, [vp, vp, i, pd]),
         "wl_momentum_kinetic": (i, [vp, vp, i, pd]),
         "wl_pion_correlator": (i, [vp, vp, i, i, pd]),
+        "wl_random_spinor": (i, [vp, ctypes.c_uint64, ctypes.c_uint64, i, vp]),
+        "wl_field_dots": (i, [vp, i, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int64, pd]),
+        "wl_field_combine": (i, [vp, i, ctypes.POINTER(vp), pd, ctypes.c_int64, vp]),
+        "wl_random_algebra": (i, [vp, ctypes.c_uint64, ctypes.c_uint64, i, d, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -313,6 +320,57 @@ class WilsonContext:
                                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
+    def field_dots(self, pairs) -> np.ndarray:
+        """<a, b> = sum conj(a) b for each (a, b) in `pairs` (complex128 device
+        tensors of equal size), in one pass per pair on the device (wl_field_dots)."""
+        pairs = [(_c128(a, self.device), _c128(b, self.device)) for a, b in pairs]
+        n = len(pairs)
+        out = np.zeros(2 * n, dtype=np.float64)
+        length = pairs[0][0].numel()
+        if any(a.numel() != length or b.numel() != length for a, b in pairs):
+            raise ValueError("field_dots: fields of different sizes")
+        A = (ctypes.c_void_p * n)(*[_ptr(a) for a, _ in pairs])
+        B = (ctypes.c_void_p * n)(*[_ptr(b) for _, b in pairs])
+        self._check(self.lib.wl_field_dots(self.handle, n, A, B, int(length),
+                                           out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out[0::2] + 1j * out[1::2]
+
+    def field_combine(self, coefs, xs, out=None):
+        """out = sum_k coefs[k] xs[k] (complex coefficients) on the device (wl_field_combine)."""
+        import torch
+
+        xs = [_c128(x, self.device) for x in xs]
+        n = len(xs)
+        c = np.empty(2 * n, dtype=np.float64)
+        c[0::2] = np.real(np.asarray(coefs, dtype=np.complex128))
+        c[1::2] = np.imag(np.asarray(coefs, dtype=np.complex128))
+        if out is None:
+            out = torch.empty_like(xs[0])
+        X = (ctypes.c_void_p * n)(*[_ptr(x) for x in xs])
+        self._check(self.lib.wl_field_combine(self.handle, n, X, c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                              int(xs[0].numel()), _ptr(out)))
+        return out
+
+    def random_spinor(self, n: int, seed: int, stream: int):
+        """n complex Gaussian fields [n, *L, 4, 3], E|z|^2 = 1, from the device
+        generator (wl_random_spinor); (seed, stream) fixes the field."""
+        import torch
+
+        out = torch.empty((int(n), *self.lattice_shape, 4, 3), dtype=torch.complex128, device=self.device)
+        self._check(self.lib.wl_random_spinor(self.handle, int(seed) & (2**64 - 1), int(stream) & (2**64 - 1),
+                                              int(n), _ptr(out)))
+        return out
+
+    def random_algebra(self, batch: int, seed: int, stream: int, scale: float = 1.0):
+        """TA(scale (G1 + i G2)) per link, [batch, 4, *L, 3, 3] (BMXYIJ), from the
+        device generator (wl_random_algebra)."""
+        import torch
+
+        out = torch.empty((int(batch), 4, *self.lattice_shape, 3, 3), dtype=torch.complex128, device=self.device)
+        self._check(self.lib.wl_random_algebra(self.handle, int(seed) & (2**64 - 1), int(stream) & (2**64 - 1),
+                                               int(batch), float(scale), _ptr(out)))
+        return out
+
     def pion_correlator(self, prop, source_t: int) -> np.ndarray:
         """C(dt), dt = 0..Lt-1, of point-source propagator columns prop [ncol, *L, 4, 3]
         (measurements.py:375-390): sum of |S|^2 over columns, spin, colour and the timeslice."""
@@ -423,6 +481,25 @@ class Engine:
         na = ctypes.c_int()
         self.ctx._check(self.ctx.lib.wl_engine_poll(self.handle, st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                                                     ctypes.byref(na)))
+        self._inputs = []
+        return st, int(na.value)
+
+    def poll_async(self):
+        """Queue the status copies behind the engine's queued work; returns at once."""
+        self.ctx._check(self.ctx.lib.wl_engine_poll_async(self.handle))
+
+    def poll_ready(self):
+        """(status, n_active) of the last poll_async once its copies have landed, else None.
+        Never blocks."""
+        st = np.zeros(self.nslots, dtype=np.int32)
+        na = ctypes.c_int()
+        r = self.ctx.lib.wl_engine_poll_ready(self.handle, st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                              ctypes.byref(na))
+        if r == 0:
+            return None
+        if r < 0:
+            raise WilsonError(WL_ERR_CUDA if r == -2 else WL_ERR_STATE,
+                              "wl_engine_poll_ready: " + ("CUDA error" if r == -2 else "no poll queued"))
         self._inputs = []
         return st, int(na.value)
 

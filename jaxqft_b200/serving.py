@@ -206,24 +206,39 @@ class PropagatorServer:
 
     # ------------------------------------------------------------------ main loop
     def run(self, requests: Sequence[Request], time_fn=time.perf_counter) -> List[Request]:
-        """Serve `requests` (arrival times in seconds from the start)."""
+        """Serve `requests` (arrival times in seconds from the start).
+
+        The host never waits on one engine while another could work: every busy
+        engine with nothing queued gets `iters_per_poll` CG iterations and a
+        non-blocking status poll on its own stream (wl_engine_poll_async); the loop
+        then admits arrivals, and handles each engine whose poll has landed
+        (wl_engine_poll_ready) by retiring its converged slots and queueing its next
+        iterations.  `self.trace` samples (seconds, queued requests, busy slots)."""
         pending = collections.deque(sorted(requests, key=lambda r: r.t_arrive))
         t0 = time_fn()
-        while pending or self.queue or any(e.owner for e in self.engines.values()):
+        inflight = set()
+        self.trace = []
+        next_sample = 0.0
+        while pending or self.queue or inflight or any(e.owner for e in self.engines.values()):
             now = time_fn() - t0
             while pending and pending[0].t_arrive <= now:
                 self.queue.append(pending.popleft())
             if self.queue:
                 self._try_admit(now)
-            busy = [e for e in self.engines.values() if e.owner]
-            if not busy:
-                if pending:
-                    time.sleep(max(0.0, min(pending[0].t_arrive - (time_fn() - t0), 0.01)))
-                continue
-            for e in busy:  # queue iterations on every engine's stream before any sync
-                e.engine.step(self.iters_per_poll)
-            for e in busy:
-                st, _ = e.engine.poll()
+            for key, e in self.engines.items():
+                if e.owner and key not in inflight:
+                    e.engine.step(self.iters_per_poll)
+                    e.engine.poll_async()
+                    inflight.add(key)
+            landed = False
+            for key in list(inflight):
+                e = self.engines[key]
+                r = e.engine.poll_ready()
+                if r is None:
+                    continue
+                inflight.discard(key)
+                landed = True
+                st, _ = r
                 for s in list(e.owner):
                     if st[s] >= L.SLOT_CONVERGED:
                         req, i = e.owner.pop(s)
@@ -235,6 +250,14 @@ class PropagatorServer:
                                 self._measure_pion(req)
                             req.t_done = time_fn() - t0
                             self.done.append(req)
+            if now >= next_sample:
+                self.trace.append((now, len(self.queue), sum(len(e.owner) for e in self.engines.values())))
+                next_sample = now + 0.05
+            if not landed:
+                if not inflight and pending:
+                    time.sleep(max(0.0, min(pending[0].t_arrive - (time_fn() - t0), 0.01)))
+                else:
+                    time.sleep(5e-5)  # the device is working; check again shortly
         if self.device.type == "cuda":
             torch.cuda.synchronize(self.device)
         return self.done
@@ -274,6 +297,19 @@ def poisson_requests(rate: float, duration: float, volumes, kappa_range=(0.120, 
     return out
 
 
+def queue_summary(trace, arrival_window: float, points: int = 40) -> dict:
+    """Queue length over time from PropagatorServer.trace: the largest queue, the
+    queue when arrivals stop, and up to `points` (seconds, queued, busy slots) samples."""
+    if not trace:
+        return {"max_queued": 0, "queued_at_window_end": 0, "samples": []}
+    t = np.array([s[0] for s in trace])
+    q = np.array([s[1] for s in trace])
+    k = int(np.searchsorted(t, arrival_window, side="right")) - 1
+    pick = np.unique(np.linspace(0, len(trace) - 1, min(points, len(trace))).astype(int))
+    return {"max_queued": int(q.max()), "queued_at_window_end": int(q[max(k, 0)]),
+            "samples": [[round(float(trace[i][0]), 3), int(trace[i][1]), int(trace[i][2])] for i in pick]}
+
+
 def summarize(done: Sequence[Request], wall: float) -> dict:
     lat = np.array([r.latency_ms for r in done])
     nsol = sum(r.nrhs for r in done)
@@ -289,3 +325,55 @@ def summarize(done: Sequence[Request], wall: float) -> dict:
             "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
             "mean_ms": float(lat.mean()) if len(lat) else None, "max_true_res": res, "all_converged": conv,
             "per_volume": per_vol}
+
+
+VOLUMES = [(8, 8, 8, 8), (12, 12, 12, 24), (16, 16, 16, 32), (24, 24, 24, 48)]
+
+
+def serve_once(server: PropagatorServer, rate: float, seconds: float, seed: int = 1) -> dict:
+    """One Poisson stream against a warm server: latency percentiles, throughput
+    and the queue length over time (the queue at the end of the arrival window
+    tells whether the rate is sustained)."""
+    server.done = []
+    reqs = poisson_requests(rate, seconds, VOLUMES, seed=seed)
+    t0 = time.perf_counter()
+    done = server.run(reqs)
+    wall = time.perf_counter() - t0
+    s = summarize(done, wall)
+    last_arrival = max((r.t_arrive for r in reqs), default=0.0)
+    last_done = max((r.t_done for r in done), default=0.0)
+    s.update({"rate_per_s": rate, "arrival_window_s": seconds, "drain_s": max(0.0, last_done - last_arrival),
+              "queue": queue_summary(server.trace, seconds)})
+    return s
+
+
+def warm_server(server: PropagatorServer, gauge_seeds=(0, 1, 2, 3)) -> None:
+    """Server start-up: one 1-RHS request per (volume, gauge field) allocates,
+    tunes and graph-captures every engine before any timed stream."""
+    warm = [Request(rid=-1 - i, volume=tuple(v), gauge=g, kappa=0.125, nrhs=1, kind="gaussian", t_arrive=0.0,
+                    seed=99 + i)
+            for i, (v, g) in enumerate((v, g) for v in VOLUMES for g in gauge_seeds)]
+    server.run(warm)
+    server.done = []
+
+
+def main(argv=None):
+    """python -m jaxqft_b200.serving --rates 50 --seconds 30   (one JSON line per rate)"""
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="Poisson propagator-request streams against a warm server")
+    ap.add_argument("--rates", default="50", help="comma-separated mean arrival rates (requests/s)")
+    ap.add_argument("--seconds", type=float, default=30.0, help="arrival window per rate")
+    ap.add_argument("--inner", default="half")
+    args = ap.parse_args(argv)
+    server = PropagatorServer(VOLUMES, gauge_seeds=(0, 1, 2, 3), nslots=16, inner=args.inner)
+    warm_server(server)
+    for rate in (float(r) for r in args.rates.split(",")):
+        s = serve_once(server, rate, args.seconds)
+        print(json.dumps({"serve": True, **s}), flush=True)
+    server.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -37,44 +37,74 @@ def _field_norm(x: torch.Tensor) -> torch.Tensor:
     return torch.sqrt(_vdot(x, x).real)
 
 
-def _chrono_predict(history: List[torch.Tensor], mode: str, max_hist: int) -> Optional[torch.Tensor]:
+class _TensorAlgebra:
+    """Inner products and linear combinations of the predictors as plain tensor
+    algebra (any torch device; the CPU tests of the predictors use it)."""
+
+    @staticmethod
+    def dots(pairs) -> np.ndarray:
+        return np.array([complex(_vdot(a, b)) for a, b in pairs], dtype=np.complex128)
+
+    @staticmethod
+    def combine(coefs, xs) -> torch.Tensor:
+        out = torch.zeros_like(xs[0])
+        for c, x in zip(coefs, xs):
+            out = out + complex(c) * x
+        return out
+
+
+class _DeviceAlgebra:
+    """The same on the library's kernels (wl_field_dots: all inner products of a
+    predictor in one launch, one pass per pair; wl_field_combine: a combination
+    in one pass)."""
+
+    def __init__(self, ctx: L.WilsonContext):
+        self.ctx = ctx
+
+    def dots(self, pairs) -> np.ndarray:
+        return self.ctx.field_dots(pairs)
+
+    def combine(self, coefs, xs) -> torch.Tensor:
+        return self.ctx.field_combine(coefs, xs)
+
+
+def _chrono_predict(history: List[torch.Tensor], mode: str, max_hist: int, la=None) -> Optional[torch.Tensor]:
     """Initial-guess extrapolation from previous solutions (su3_wilson_nf2.py:85-111):
     'last' or the uniform-step polynomial sum_j (-1)^j C(p, j+1) x_{k-j}."""
     if not history:
         return None
+    la = _TensorAlgebra if la is None else la
     h = history[-max(1, int(max_hist)):]
     if len(h) == 1 or mode == "last":
         return h[-1]
     p = len(h)
-    x0 = torch.zeros_like(h[-1])
-    for j in range(p):
-        x0 = x0 + float(((-1) ** j) * math.comb(p, j + 1)) * h[-1 - j]
-    return x0
+    return la.combine([float(((-1) ** j) * math.comb(p, j + 1)) for j in range(p)], [h[-1 - j] for j in range(p)])
 
 
 def _chrono_predict_mre(xs: List[torch.Tensor], ys: List[torch.Tensor], target: torch.Tensor,
-                        reg: float = 1e-12) -> Optional[torch.Tensor]:
+                        reg: float = 1e-12, la=None) -> Optional[torch.Tensor]:
     """Minimal-residual extrapolation (su3_wilson_nf2.py:114-194): with history
     pairs (x_i, y_i = L x_i), minimise ||target - sum_i c_i y_i|| over c with
     older entries damped by exp(-0.35 age), Tikhonov regularisation reg*tr(G)/n,
     and the reference's safeguards (coefficient bounds, trust-region blend
     towards x_last, norm growth limit, and acceptance only if the subspace
-    residual beats the latest image by 3 %).  Inner products run on the device;
-    the n x n solve on the host, as in the reference."""
+    residual beats the latest image by 3 %).  Inner products and combinations
+    run through `la` (the device kernels in the theory); the n x n solve on the
+    host, as in the reference."""
     if not xs or not ys:
         return None
     if len(xs) == 1:
         return xs[-1]
+    la = _TensorAlgebra if la is None else la
     n = len(xs)
     w = np.asarray([math.exp(-0.35 * float((n - 1) - i)) for i in range(n)])
+    upper = [(i, j) for i in range(n) for j in range(i, n)]
+    d = la.dots([(ys[i], target) for i in range(n)] + [(ys[i], ys[j]) for i, j in upper])
+    g = w * d[:n]
     G = np.zeros((n, n), dtype=np.complex128)
-    g = np.zeros((n,), dtype=np.complex128)
-    for i in range(n):
-        g[i] = w[i] * complex(_vdot(ys[i], target))
-        for j in range(i, n):
-            gij = w[i] * w[j] * complex(_vdot(ys[i], ys[j]))
-            G[i, j] = gij
-            G[j, i] = np.conj(gij)
+    for (i, j), v in zip(upper, d[n:]):
+        G[i, j] = w[i] * w[j] * v
+        G[j, i] = np.conj(G[i, j])
     lam = float(reg) * max(1.0, abs(float(np.trace(G).real)) / max(1, n))
     Greg = G + lam * np.eye(n, dtype=np.complex128)
     try:
@@ -87,40 +117,21 @@ def _chrono_predict_mre(xs: List[torch.Tensor], ys: List[torch.Tensor], target: 
     cmax, cl1 = float(np.max(np.abs(c))), float(np.sum(np.abs(c)))
     if cmax > 2.0 or cl1 > 3.0:
         return xs[-1]
-    x0 = torch.zeros_like(xs[-1])
-    for ci, xi in zip(c, xs):
-        x0 = x0 + complex(ci) * xi
+    # x0 = beta sum_i c_i x_i + (1 - beta) x_last, in one combination
     beta = 1.0 / max(1.0, cl1)
-    x0 = beta * x0 + (1.0 - beta) * xs[-1]
-    n_last, n_x0 = float(_field_norm(xs[-1])), float(_field_norm(x0))
+    cx = beta * c
+    cx[-1] += 1.0 - beta
+    x0 = la.combine(list(cx), xs)
+    # target - sum_i c_i y_i and target - y_last
+    r_comb = la.combine([1.0] + list(-c), [target] + list(ys))
+    r_last = la.combine([1.0, -1.0], [target, ys[-1]])
+    nn = la.dots([(xs[-1], xs[-1]), (x0, x0), (r_comb, r_comb), (r_last, r_last)]).real
+    n_last, n_x0, r_mre, r_lst = (math.sqrt(max(v, 0.0)) if math.isfinite(v) else float("nan") for v in nn)
     if not math.isfinite(n_x0) or (n_last > 0.0 and n_x0 > 5.0 * n_last):
         return xs[-1]
-    y_comb = torch.zeros_like(ys[-1])
-    for ci, yi in zip(c, ys):
-        y_comb = y_comb + complex(ci) * yi
-    r_mre, r_last = float(_field_norm(target - y_comb)), float(_field_norm(target - ys[-1]))
-    if not (math.isfinite(r_mre) and math.isfinite(r_last)) or r_mre >= 0.97 * r_last:
+    if not (math.isfinite(r_mre) and math.isfinite(r_lst)) or r_mre >= 0.97 * r_lst:
         return xs[-1]
     return x0
-
-
-@dataclass
-class GaugeActionMonomial:
-    """Plaquette monomial (su3_wilson_nf2.py:197-214)."""
-
-    model: "SU3WilsonNf2"
-    name: str = "gauge"
-    timescale: int = 0
-    stochastic: bool = False
-
-    def refresh(self, q, traj_length: float = 1.0) -> None:
-        return None
-
-    def action(self, q):
-        return SU3YangMills.action(self.model, q)
-
-    def force(self, q):
-        return SU3YangMills.force(self.model, q)
 
 
 @dataclass
@@ -158,11 +169,12 @@ class _PFBase:
             pairs = [(x, y) for x, y in zip(self._hist[-keep:], self._img[-keep:])
                      if y is not None and y.shape == self.eta.shape]
             if pairs:
-                x0 = _chrono_predict_mre([p[0] for p in pairs], [p[1] for p in pairs], self.eta)
+                x0 = _chrono_predict_mre([p[0] for p in pairs], [p[1] for p in pairs], self.eta,
+                                         la=_DeviceAlgebra(m.ctx))
                 if x0 is not None:
                     return x0
             mode = "poly"  # no images / no eta (OU refresh): polynomial fallback
-        return _chrono_predict(self._hist, "poly" if mode == "poly" else "last", keep)
+        return _chrono_predict(self._hist, "poly" if mode == "poly" else "last", keep, la=_DeviceAlgebra(m.ctx))
 
     def _remember(self, x, y=None):
         if self.model.use_solver_guess:
@@ -503,9 +515,9 @@ class SU3WilsonNf2(SU3YangMills):
 
     # ------------------------------------------------------------------ random fields
     def random_fermion(self):
-        """Complex Gaussian with E|z|^2 = 1 (su3_wilson_nf2.py:1169-1175)."""
-        shp = self.fermion_shape()
-        return self._out(torch.complex(self._randn(shp), self._randn(shp)) / math.sqrt(2.0))
+        """Complex Gaussian with E|z|^2 = 1 (su3_wilson_nf2.py:1169-1175), drawn by the
+        device generator (wl_random_spinor) with the theory's seed and a fresh stream."""
+        return self._out(self.ctx.random_spinor(self.Bs, self.seed, self._next_stream()))
 
     def sample_pseudofermion(self, U):
         return self.apply_Ddag(U, self.random_fermion())
@@ -547,14 +559,40 @@ class SU3WilsonNf2(SU3YangMills):
         return self._solve("eo_normal", U, self._project_even(rhs), self._project_even(x0))
 
     # Non-Hermitian solves (:1271-1454).  The reference runs BiCGStab / GMRES on D (or on the
-    # Schur operator); here every one of them is the batched mixed-precision CG on the normal
-    # equations of the same operator (CGNR): A x = b  <=>  A^dag A x = A^dag b, and
-    # A^dag y = b  <=>  y = A (A^dag A)^-1 b.  The solution is the same to solver tolerance;
-    # ``cg_tol`` bounds the normal-equation residual.  ``solver_kind`` bicgstab / gmres and
-    # ``gmres_restart`` are accepted for configuration compatibility and select the same CGNR.
+    # Schur operator) and stops at ||b - A x|| <= cg_tol ||b|| (relative, atol 0).  Here every one
+    # of them is the batched mixed-precision CG on the normal equations of the same operator
+    # (CGNR), held to that same stopping rule:
+    #   A^dag y = b  <=>  y = A z with A^dag A z = b: the residual b - A^dag y is the normal
+    #     residual of z, which CG bounds by cg_tol, so the rule holds as it is;
+    #   A x = b  <=>  A^dag A x = A^dag b: CG bounds ||A^dag (b - A x)|| only, so x is refined by
+    #     defect correction (_refine_direct) until the FP64 residual ||b - A x|| meets the rule.
+    # ``solver_kind`` bicgstab / gmres and ``gmres_restart`` are accepted for configuration
+    # compatibility and select the same solver.
+    max_refine_rounds = 8  # defect-correction rounds of a direct solve (a class constant)
+
+    def _refine_direct(self, apply_A, solve_normal_eq, b: torch.Tensor, tol: Optional[float]) -> torch.Tensor:
+        """x with ||b - A x|| <= tol ||b|| for every batch entry.  solve_normal_eq(r) returns
+        the CGNR solution of A x = r; each round solves for the current FP64 residual and adds
+        the correction, which shrinks the residual by about cond(A) * tol."""
+        tol = self.cg_tol if tol is None else float(tol)
+        x = solve_normal_eq(b)
+        bn = torch.stack([_field_norm(b[i]) for i in range(b.shape[0])])
+        for _ in range(int(self.max_refine_rounds)):
+            r = b - apply_A(x)
+            rn = torch.stack([_field_norm(r[i]) for i in range(r.shape[0])])
+            if bool(torch.all(rn <= tol * bn)):
+                return x
+            x = x + solve_normal_eq(r)
+        warnings.warn(f"direct residual did not reach tol {tol} in {self.max_refine_rounds} refinements",
+                      RuntimeWarning)
+        return x
+
     def solve_direct(self, U, rhs, tol: Optional[float] = None):
-        """x = D^-1 rhs (:1271-1284)."""
-        return self._out(self._solve_raw("normal", U, self._apply_raw("DDAG", U, rhs), tol=tol))
+        """x = D^-1 rhs (:1271-1284), ||rhs - D x|| <= cg_tol ||rhs||."""
+        b = self._as_tensor(rhs)
+        return self._out(self._refine_direct(
+            lambda x: self._apply_raw("D", U, x),
+            lambda r: self._solve_raw("normal", U, self._apply_raw("DDAG", U, r), tol=tol), b, tol))
 
     def solve_dagger(self, U, rhs, tol: Optional[float] = None):
         """y = D^-dag rhs (:1286-1299)."""
@@ -573,8 +611,7 @@ class SU3WilsonNf2(SU3YangMills):
         b_e, b_o = self._project_even(b), self._project_odd(b)
         rhs_e = b_e - self._project_even(self._apply_raw(op, U, b_o) - m0 * b_o) / m0
         if which == "direct":  # M x_e = rhs_e / m0  <=>  M^dag M x_e = M^dag rhs_e / m0
-            rhs_n = self._apply_raw("SCHUR_E_DAG", U, rhs_e / m0, normalized=True)
-            x_e = self._project_even(self._solve_raw("eo_normal", U, rhs_n, tol=tol))
+            x_e = self._solve_schur_direct(U, rhs_e / m0, tol)
         else:  # M^dag x_e = rhs_e / m0  <=>  x_e = M (M^dag M)^-1 rhs_e / m0
             z_e = self._project_even(self._solve_raw("eo_normal", U, rhs_e / m0, tol=tol))
             x_e = self._project_even(self._apply_raw("SCHUR_E", U, z_e, normalized=True))
@@ -587,10 +624,19 @@ class SU3WilsonNf2(SU3YangMills):
     def solve_dagger_eo(self, U, rhs, tol: Optional[float] = None):
         return self._out(self._solve_eo(U, rhs, "dagger", tol))
 
+    def _solve_schur_direct(self, U, rhs_e, tol: Optional[float]) -> torch.Tensor:
+        """x_e with ||rhs_e - M x_e|| <= tol ||rhs_e||, M the normalized even Schur operator
+        (the rule of _solve_eo_one and solve_eop_even_direct, scale-free, so it also holds for
+        the unnormalized m0 M)."""
+        return self._refine_direct(
+            lambda x: self._project_even(self._apply_raw("SCHUR_E", U, x, normalized=True)),
+            lambda r: self._project_even(self._solve_raw(
+                "eo_normal", U, self._apply_raw("SCHUR_E_DAG", U, r, normalized=True), tol=tol)),
+            self._project_even(rhs_e), tol)
+
     def solve_eop_even_direct(self, U, rhs, tol: Optional[float] = None):
         """M x_e = rhs_e, M the normalized even Schur operator (:1338-1350)."""
-        rhs_n = self._apply_raw("SCHUR_E_DAG", U, self._project_even(rhs), normalized=True)
-        return self._out(self._project_even(self._solve_raw("eo_normal", U, rhs_n, tol=tol)))
+        return self._out(self._solve_schur_direct(U, self._as_tensor(rhs), tol))
 
     def solve_eop_even_dagger(self, U, rhs, tol: Optional[float] = None):
         """M^dag y_e = rhs_e (:1352-1364)."""

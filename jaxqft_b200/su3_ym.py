@@ -47,7 +47,6 @@ class SU3YangMills:
     exp_method: str = "expm"
     dtype: torch.dtype = torch.complex128
     device: Optional[str] = None
-    generator: torch.Generator = field(init=False, repr=False)
 
     _wl: Optional[object] = field(init=False, default=None, repr=False)
 
@@ -65,8 +64,7 @@ class SU3YangMills:
             raise RuntimeError("the B200 Wilson-fermion path requires a CUDA device (no CPU fallback)")
         self.device = torch.device(self.device) if self.device is not None else torch.device(
             "cuda", torch.cuda.current_device())
-        self.generator = torch.Generator(device=self.device)
-        self.generator.manual_seed(int(self.seed))
+        self._rng_stream = 0  # draws of the device generator so far (one stream each)
         self.mu_axis = 1 if self.layout == "BMXYIJ" else 1 + self.Nd
 
     # ------------------------------------------------------------------ layout
@@ -90,14 +88,18 @@ class SU3YangMills:
         return x.select(self.mu_axis, mu)
 
     # ------------------------------------------------------------------ random fields
-    def _randn(self, shape):
-        return torch.randn(shape, generator=self.generator, device=self.device, dtype=torch.float64)
+    def _next_stream(self) -> int:
+        """Stream number of the next device-generator draw: each draw of the
+        theory uses a fresh stream of the theory's seed, as the reference splits
+        a fresh jax.random key per draw (su3_ym.py:234-236)."""
+        self._rng_stream += 1
+        return self._rng_stream
 
     def _sample_algebra(self, scale: float = 1.0) -> torch.Tensor:
-        """TA(scale (G1 + i G2)) with Gaussian G (su3_ym.py:238-244)."""
-        shp = self.field_shape()
-        a = scale * torch.complex(self._randn(shp), self._randn(shp)).to(self.dtype)
-        return project_su3_algebra(a)
+        """TA(scale (G1 + i G2)) with Gaussian G (su3_ym.py:238-244), drawn by the
+        device generator (wl_random_algebra)."""
+        P = self._ctx().random_algebra(self.Bs, self.seed, self._next_stream(), scale)
+        return self._from_bm(P).to(self.dtype)
 
     def algebra_to_links(self, q: torch.Tensor) -> torch.Tensor:
         return torch.linalg.matrix_exp(project_su3_algebra(q))

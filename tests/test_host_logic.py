@@ -93,6 +93,14 @@ class FakeEngine:
             st[s] = serving.L.SLOT_CONVERGED if k == 0 else 1
         return st, sum(1 for k in self.left.values() if k > 0)
 
+    def poll_async(self):
+        # the copies "land" on the second readiness check: the loop must cope with a poll in flight
+        self._snap, self._checks = self.poll(), 0
+
+    def poll_ready(self):
+        self._checks += 1
+        return self._snap if self._checks >= 2 else None
+
     def retire(self, s, out=None):
         assert self.left.pop(s) == 0
         return out, {"iters": 10, "status": serving.L.SLOT_CONVERGED, "true_res": 1e-11, "reliable_updates": 1}
@@ -160,6 +168,17 @@ def test_serving_continuous_batching_shares_an_engine(fake_engines):
     assert fake_engines.created[0].max_busy == 8
     summ = serving.summarize(done, wall=1.0)
     assert summ["solves"] == 8 and summ["all_converged"] and summ["requests"] == 2
+
+
+def test_serving_trace_and_queue_summary(fake_engines):
+    srv = make_server([VOL], nslots=4, budget=10**9, engine_bytes=100)
+    reqs = [serving.Request(rid=i, volume=VOL, gauge=0, kappa=0.125, nrhs=3, kind="point", t_arrive=0.0)
+            for i in range(3)]
+    srv.run(reqs, time_fn=FakeClock(1e-2))
+    assert srv.trace and srv.trace[0][1] >= 1  # requests queued at the start
+    q = serving.queue_summary(srv.trace, arrival_window=0.0, points=5)
+    assert q["max_queued"] >= 1 and len(q["samples"]) <= 5
+    assert serving.queue_summary([], 1.0)["max_queued"] == 0
 
 
 def test_serving_waits_for_free_slots(fake_engines):
