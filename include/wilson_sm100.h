@@ -211,8 +211,10 @@ int64_t wl_bounds_errors(long long* first_bad);
    2 * nrhs * volume * 192 bytes must fit (nrhs * volume <= 174762, e.g. one
    16^3x32 field); larger requests return WL_ERR_ARG.  The first call on a
    device resolves the array's address with that device current; make it
-   before any stream capture.  All calls share the array: calls that overlap
-   on the GPU (different streams or contexts of one device) race. */
+   before any stream capture.  The address is kept for the life of the
+   process, so the library must not be used across a cudaDeviceReset of that
+   device.  All calls share the array: calls that overlap on the GPU
+   (different streams or contexts of one device) race. */
 wl_status wl_apply_schur_normal_noalloc(wl_ctx* ctx, wl_gauge* gauge, double mass, unsigned flags,
                                         const void* in, void* out, int nrhs);
 

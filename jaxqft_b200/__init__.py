@@ -15,7 +15,7 @@ def __getattr__(name):
     import importlib
 
     if name in ("lib", "build", "gamma", "su3_ym", "su3_wilson_nf2", "update", "integrators", "hamiltonian",
-                "serving", "wilson", "measurements", "lime", "hmc_run"):
+                "serving", "wilson", "measurements", "lime", "hmc_run", "hmc_compare", "stats"):
         return importlib.import_module(f".{name}", __name__)
     if name == "SU3WilsonNf2":
         return importlib.import_module(".su3_wilson_nf2", __name__).SU3WilsonNf2

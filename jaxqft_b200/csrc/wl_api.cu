@@ -2319,8 +2319,9 @@ static std::mutex g_noalloc_mu;
 static void* g_noalloc_ptr[64] = {nullptr};
 
 // Device address of the scratch array for ctx->device.  Resolved once per
-// device (with that device current) and cached; host code must never use the
-// symbol itself as a device pointer.
+// device (with that device current) and cached for the life of the process, so
+// the library must not be used across a cudaDeviceReset of that device; host
+// code must never use the symbol itself as a device pointer.
 static wl_status noalloc_scratch(wl_ctx* ctx, void** out) {
   if (ctx->device < 0 || ctx->device >= 64) WL_FAIL(ctx, WL_ERR_ARG, "device ordinal out of range");
   std::lock_guard<std::mutex> lk(g_noalloc_mu);

@@ -81,6 +81,10 @@ def _chrono_predict(history: List[torch.Tensor], mode: str, max_hist: int, la=No
     return la.combine([float(((-1) ** j) * math.comb(p, j + 1)) for j in range(p)], [h[-1 - j] for j in range(p)])
 
 
+# _chrono_predict_mre condenses _chrono_predict_mre of jaxqft/models/su3_wilson_nf2.py:114-194
+# (jaxQFT, BSD 3-Clause License, Copyright (c) 2026, Kostas Orginos; the full notice is in
+# jaxqft_b200/update.py): its damping, regularisation and safeguard steps and constants are the
+# reference's, since the predictor must reproduce the reference's initial guesses.
 def _chrono_predict_mre(xs: List[torch.Tensor], ys: List[torch.Tensor], target: torch.Tensor,
                         reg: float = 1e-12, la=None) -> Optional[torch.Tensor]:
     """Minimal-residual extrapolation (su3_wilson_nf2.py:114-194): with history
@@ -685,13 +689,47 @@ class SU3WilsonNf2(SU3YangMills):
                 "mean_abs_residual": float(absn.mean()), "max_abs_residual": float(absn.max())}
 
     def solver_info_stats(self, U, phi) -> Dict[str, float]:
-        """Per-RHS iteration counts of a normal solve (real counts: the reference's
-        JAX cg reports none, su3_wilson_nf2.py:1459-1545)."""
-        self.solve_normal(U, phi)
-        it = np.asarray([s["iters"] for s in self.last_solver_stats], dtype=np.float64)
+        """Per-RHS iteration counts (su3_wilson_nf2.py:1468-1554): the solve of the
+        configured form is run and its CG iterations counted -- for "normal" one
+        normal-equation solve per configuration; for "split" / "eo_split" stage 1
+        A^dag y = phi and stage 2 A x = y (the direct stage including its
+        defect-correction rounds), reported as the stage means and their sum.  The
+        counts are real (the reference's JAX solvers report none, so its
+        iters_known_fraction is 0 there)."""
+        phi = self._as_tensor(phi)
+        counts: List[List[int]] = []
+        orig = self._solve_raw
+
+        def counting(*a, **k):
+            out = orig(*a, **k)
+            counts.append([int(st["iters"]) for st in self.last_solver_stats])
+            return out
+
+        self._solve_raw = counting
+        try:
+            B = phi.shape[0]
+            if self.solver_form == "normal":
+                self.solve_normal(U, phi)
+                it = np.asarray(counts[-1], dtype=np.float64)
+                it1 = it2 = None
+            else:
+                eo = self.solver_form == "eo_split"
+                counts.clear()
+                y = self._solve_eo(U, phi, "dagger") if eo else self.solve_dagger(U, phi)
+                it1 = np.sum(np.asarray(counts, dtype=np.float64).reshape(len(counts), B), axis=0)
+                counts.clear()
+                if eo:
+                    self._solve_eo(U, y, "direct")
+                else:
+                    self.solve_direct(U, y)
+                it2 = np.sum(np.asarray(counts, dtype=np.float64).reshape(len(counts), B), axis=0)
+                it = it1 + it2
+        finally:
+            del self._solve_raw
         return {"iters_known_fraction": 1.0, "mean_solver_iters": float(it.mean()),
-                "max_solver_iters": float(it.max()), "mean_solver_iters_stage1": float("nan"),
-                "mean_solver_iters_stage2": float("nan")}
+                "max_solver_iters": float(it.max()),
+                "mean_solver_iters_stage1": float(it1.mean()) if it1 is not None else float("nan"),
+                "mean_solver_iters_stage2": float(it2.mean()) if it2 is not None else float("nan")}
 
     # ------------------------------------------------------------------ actions (:1183-1208)
     def _split_chi(self, U, phi, eo_prec: bool, tol: Optional[float] = None) -> torch.Tensor:

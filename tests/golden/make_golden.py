@@ -1,7 +1,7 @@
 """Generate golden input/output vectors by running the reference's own code.
 
-Run in a container where the jaxQFT sources are mounted (default location
-``/root/reference``; override with ``--ref``).  The reference modules are
+Run where the jaxQFT sources are available (pass their root with ``--ref``).
+The reference modules are
 imported unchanged under the numpy JAX shim (``_shim/jax``, see
 ``reference_loader.py``) with ``dtype=complex128``, so every output below is
 what the reference's algorithm computes in FP64 on the stored inputs.
@@ -13,7 +13,7 @@ what ``SU3YangMills.hot_start(scale=a)`` computes (jaxqft/models/su3_ym.py:238-
 ``random_fermion`` (jaxqft/models/su3_wilson_nf2.py:1169-1175).
 
 Output: ``golden_<case>.npz`` beside this script.  Usage:
-    python tests/golden/make_golden.py [--ref /path/to/jaxQFT]
+    python tests/golden/make_golden.py --ref /path/to/jaxQFT
 """
 
 from __future__ import annotations
@@ -239,7 +239,7 @@ def run_lime(ref_root):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the jaxQFT source tree")
     args = ap.parse_args()
     from reference_loader import load_reference
 

@@ -75,3 +75,23 @@ def test_device_predictors_match_reference():
     d = la.dots([(xs[0], ys[1]), (ys[2], ys[2])])
     assert abs(d[0] - np.vdot(g["xs"][0], g["ys"][1])) < 1e-12 * abs(d[0])
     assert abs(d[1] - np.vdot(g["ys"][2], g["ys"][2])) < 1e-12 * abs(d[1])
+
+
+def test_device_predictors_match_reference():
+    """The predictors on the library's kernels (wl_field_dots / wl_field_combine)
+    against the reference's own outputs (golden_chrono.npz)."""
+    from jaxqft_b200.lib import WilsonContext
+    from jaxqft_b200.su3_wilson_nf2 import _chrono_predict, _chrono_predict_mre, _DeviceAlgebra
+    from tests.conftest import load_golden
+
+    g = load_golden("chrono")
+    la = _DeviceAlgebra(WilsonContext((4, 4, 4, 4)))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    xs, ys = [t(x) for x in g["xs"]], [t(y) for y in g["ys"]]
+    assert rel(_chrono_predict(xs, "poly", 4, la=la).cpu().numpy(), g["poly"]) < 1e-14
+    assert rel(_chrono_predict(xs, "poly", 3, la=la).cpu().numpy(), g["poly3"]) < 1e-14
+    assert rel(_chrono_predict_mre(xs, ys, t(g["target"]), la=la).cpu().numpy(), g["mre"]) < 1e-12
+    assert rel(_chrono_predict_mre(xs, ys, t(g["far"]), la=la).cpu().numpy(), g["mre_far"]) < 1e-15
+    d = la.dots([(xs[0], ys[1]), (ys[2], ys[2])])
+    assert abs(d[0] - np.vdot(g["xs"][0], g["ys"][1])) < 1e-12 * abs(d[0])
+    assert abs(d[1] - np.vdot(g["ys"][2], g["ys"][2])) < 1e-12 * abs(d[1])
