@@ -139,6 +139,25 @@ def _chrono_predict_mre(xs: List[torch.Tensor], ys: List[torch.Tensor], target: 
 
 
 @dataclass
+class GaugeActionMonomial:
+    """Plaquette monomial (su3_wilson_nf2.py:197-214)."""
+
+    model: "SU3WilsonNf2"
+    name: str = "gauge"
+    timescale: int = 0
+    stochastic: bool = False
+
+    def refresh(self, q, traj_length: float = 1.0) -> None:
+        return None
+
+    def action(self, q):
+        return SU3YangMills.action(self.model, q)
+
+    def force(self, q):
+        return SU3YangMills.force(self.model, q)
+
+
+@dataclass
 class _PFBase:
     model: "SU3WilsonNf2"
     name: str = "wilson_nf2_pf"
