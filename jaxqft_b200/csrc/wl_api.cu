@@ -575,16 +575,14 @@ static wl_status ensure_tmp(wl_ctx* ctx, size_t bytes) {
 
 // Kernel for the reference-layout hop: 0 = ref_pair_kernel (two threads per
 // site, 256-bit spinor accesses, parity-split SoA links; the default),
-// 1 = row_hop_kernel (TMA row staging), 2 = hop_kernel on the reference layout,
-// 3 = ref_site_kernel (one thread per site).  WL_REF_HOP=pair|row|generic|tps
-// selects one (for comparisons).
+// 1 = row_hop_kernel (TMA row staging), 2 = hop_kernel on the reference layout.
+// WL_REF_HOP=pair|row|generic selects one (for comparisons).
 static int ref_hop_kind() {
   static const int k = [] {
     const char* e = std::getenv("WL_REF_HOP");
     if (!e) return 0;
     if (std::strcmp(e, "row") == 0) return 1;
     if (std::strcmp(e, "generic") == 0) return 2;
-    if (std::strcmp(e, "tps") == 0) return 3;
     return 0;
   }();
   return k;
@@ -659,8 +657,7 @@ template <bool DAG>
 static bool site_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const void* self, double a, double b,
                      int nrhs, int parity) {
   const Geom& g = ctx->g;
-  const int kind = ref_hop_kind();
-  if ((kind != 0 && kind != 3) || nrhs > 65535) return false;
+  if (ref_hop_kind() != 0 || nrhs > 65535) return false;
   RefSiteArgs A{};
   A.g = g;
   A.U = G->d18;
@@ -671,17 +668,12 @@ static bool site_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const 
   A.b = b;
   A.nrhs = nrhs;
   A.parity = parity;
-  const long long n = (parity < 0 ? g.V : g.Vh) * (kind == 0 ? 2LL : 1LL);  // threads per field
+  const long long n = (parity < 0 ? g.V : g.Vh) * 2LL;  // two threads per target site
   const dim3 grid((unsigned)((n + kRefSiteBlock - 1) / kRefSiteBlock), nrhs);
   const bool w32 = (((uintptr_t)in | (uintptr_t)out | (uintptr_t)self) & 31) == 0;
   g_launches++;
-  if (kind == 0) {
-    if (w32) ref_pair_kernel<DAG, 4><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
-    else ref_pair_kernel<DAG, 2><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
-  } else {
-    if (w32) ref_site_kernel<DAG, 4><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
-    else ref_site_kernel<DAG, 2><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
-  }
+  if (w32) ref_pair_kernel<DAG, 4><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
+  else ref_pair_kernel<DAG, 2><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
   return true;
 }
 

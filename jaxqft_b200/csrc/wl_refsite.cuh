@@ -1,26 +1,30 @@
-// FP64 Wilson hop on reference-layout fermions, one thread per target site,
-// for the drop-in operators (D, D^dag, K, the masked and Schur forms).
+// FP64 Wilson hop on reference-layout fermions for the drop-in operators (D,
+// D^dag, K, the masked and Schur forms): two threads per target site.
 //
 // Fermions keep the caller's layout: complex128 [rhs][Lx][Ly][Lz][Lt][4][3],
 // 192 contiguous bytes per site.  sm_100 has 256-bit global loads and stores
-// (ld.global.v4.f64 / st.global.v4.f64), so a thread moves its neighbour's
-// spinor as six 32-byte sectors: every sector a warp requests is used whole,
-// and no shared-memory staging or block barrier is needed.  For mu = 3 only the
-// two spins the projector keeps are loaded (three sectors).  Links come from the
+// (ld.global.v4.f64 / st.global.v4.f64), so a spin (48 bytes) is one 32-byte
+// vector and one 16-byte half, and a pair of threads reads a neighbour's
+// spinor without shared-memory staging or block barriers.  Links come from the
 // gauge object's parity-split SoA copy (double2 [p][mu][9][Vh]), so a warp's
-// link load is two contiguous 256-byte runs (the two parities of 16 compact
-// sites) instead of a 144-byte-stride gather.  Neighbour spinors and the second
-// use of every link (forward from x, backward from x + mu) are L2 hits: the
-// reuse distance is at most one x-slice of the lattice (Ly*Lz*Lt sites).
+// link load is two contiguous runs (the two parities of 8 compact sites)
+// instead of a 144-byte-stride gather.  Neighbour spinors and the second use
+// of every link (forward from x, backward from x + mu) are L2 hits: the reuse
+// distance is at most one x-slice of the lattice (Ly*Lz*Lt sites).
 //
-// Thread mapping: with both parities targeted (D, D^dag, K) thread i of the
-// grid row owns flat site i, so a warp covers 32 consecutive sites; with one
-// target parity p thread i owns compact site i of parity p.
+// Thread mapping: with both parities targeted (D, D^dag, K) pair i of the grid
+// row owns flat site i, so a warp covers 16 consecutive sites; with one target
+// parity p pair i owns compact site i of parity p.
 //
 // Contract = row_hop_kernel: out = a*self + b*acc on the target sites,
 //   acc = sum_mu [(1 + cf g_mu) U_mu(x) psi(x+mu) + (1 + cb g_mu) U_mu^dag(x-mu) psi(x-mu)],
 // cf = -1 (D) or +1 (D^dag), cb = -cf, boundary phase on the forward hop from
 // x_mu = L_mu - 1 and (conjugated) on the backward hop into x_mu = 0.
+//
+// Measured at 24^3x48 (1 RHS): 0.217 ms, limited by the L1 data pipe (83-88 % of
+// its wavefront rate at 33 % of DRAM bandwidth): every load instruction of a
+// warp touches one or two sectors of each of its 16 sites.  A one-thread-per-
+// site form (six 32-byte loads per neighbour, 168 registers) timed the same.
 #pragma once
 #include "wl_hop.cuh"
 
@@ -62,115 +66,7 @@ WL_D void st_vec(double* p, const double* v) {
   }
 }
 
-// reals [lo, hi) of one site's 24
-template <int W, int LO, int HI>
-WL_D void ld_site_part(const double* site, double (&v)[24]) {
-#pragma unroll
-  for (int k = LO; k < HI; k += W) ld_vec<W>(site + k, v + k);
-}
-
-template <int MU, int C, bool DAGU, int W>
-WL_D void refsite_dir(const double* src, const double2* lk, unsigned vh, bool ph, const Geom& g,
-                      Spinor<double>& acc) {
-  double v[24];
-  // mu = 3 projects onto spins (0, 1) for C > 0 and (2, 3) for C < 0: load only those
-  constexpr int lo = (MU == 3 && C < 0) ? 12 : 0;
-  constexpr int hi = (MU == 3 && C > 0) ? 12 : 24;
-  ld_site_part<W, lo, hi>(src, v);
-  Spinor<double> s;
-#pragma unroll
-  for (int k = 0; k < 12; ++k) s.v[k / 3][k % 3] = (2 * k >= lo && 2 * k < hi) ? cplx<double>{v[2 * k], v[2 * k + 1]}
-                                                                               : cplx<double>{0.0, 0.0};
-  Link<double> u;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    const double2 q = ldg(lk + (size_t)k * vh);
-    u.m[k / 3][k % 3] = {q.x, q.y};
-  }
-  Half<double> h, uh;
-  spin_project<MU, C>(s, h);
-  color_mul<DAGU>(u, h, uh);
-  if (ph) phase_mul(uh, g.ph_re[MU], DAGU ? -g.ph_im[MU] : g.ph_im[MU]);
-  spin_accum<MU, C>(acc, uh);
-}
-
-template <int MU, bool DAG, int W>
-WL_D void refsite_mu(const RefSiteArgs& A, const double* base, const Site& s, int parity, Spinor<double>& acc) {
-  constexpr int CF = DAG ? +1 : -1;
-  constexpr int CB = -CF;
-  const Geom& g = A.g;
-  const unsigned vh = (unsigned)g.Vh;
-  {  // forward: U_mu(x) psi(x+mu); the link is stored with the target site's parity
-    const int nb = neighbor(g, s, MU, +1);
-    const int tn = MU == 3 ? (s.x[3] == g.L[3] - 1 ? 0 : s.x[3] + 1) : s.x[3];
-    const double* src = base + (size_t)(2 * nb + (tn & 1)) * 24;
-    const double2* lk = A.U + (size_t)(parity * 4 + MU) * 9 * vh + s.c;
-    refsite_dir<MU, CF, false, W>(src, lk, vh, g.ph_on[MU] && s.x[MU] == g.L[MU] - 1, g, acc);
-  }
-  {  // backward: U_mu(x-mu)^dag psi(x-mu); the link is stored with the other parity
-    const int nb = neighbor(g, s, MU, -1);
-    const int tn = MU == 3 ? (s.x[3] == 0 ? g.L[3] - 1 : s.x[3] - 1) : s.x[3];
-    const double* src = base + (size_t)(2 * nb + (tn & 1)) * 24;
-    const double2* lk = A.U + (size_t)((1 - parity) * 4 + MU) * 9 * vh + nb;
-    refsite_dir<MU, CB, true, W>(src, lk, vh, g.ph_on[MU] && s.x[MU] == 0, g, acc);
-  }
-}
-
-#ifndef WL_REFSITE_MINB
-#define WL_REFSITE_MINB 3  // resident 128-thread blocks per SM the kernel is compiled for
-#endif
 constexpr int kRefSiteBlock = 128;
-
-template <bool DAG, int W>
-__global__ void __launch_bounds__(kRefSiteBlock, WL_REFSITE_MINB) ref_site_kernel(RefSiteArgs A) {
-  const Geom& g = A.g;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y;
-  Site s;
-  int parity;
-  if (A.parity < 0) {  // every site: i is the flat index
-    if (i >= g.V) return;
-    const int c = i >> 1;
-    const int row = (int)fdiv(g.fd_lth, (unsigned)c);
-    const int t = i - row * g.L[3];
-    const int r2 = (int)fdiv(g.fd_l2, (unsigned)row);
-    s.c = WL_CHECKED(c, g.Vh);
-    s.row = row;
-    s.x[2] = row - r2 * g.L[2];
-    s.x[0] = (int)fdiv(g.fd_l1, (unsigned)r2);
-    s.x[1] = r2 - s.x[0] * g.L[1];
-    s.x[3] = t;
-    parity = (s.x[0] + s.x[1] + s.x[2] + t) & 1;
-  } else {  // one parity: i is the compact index
-    if (i >= g.Vh) return;
-    parity = A.parity;
-    s = site_from_compact(g, parity, i);
-  }
-  const size_t flat = (size_t)s.row * g.L[3] + s.x[3];
-  const size_t field = (size_t)rhs * g.V * 24;
-  const double* base = A.in + field;
-  Spinor<double> acc;
-  zero(acc);
-  refsite_mu<0, DAG, W>(A, base, s, parity, acc);
-  refsite_mu<1, DAG, W>(A, base, s, parity, acc);
-  refsite_mu<2, DAG, W>(A, base, s, parity, acc);
-  refsite_mu<3, DAG, W>(A, base, s, parity, acc);
-  double o[24];
-#pragma unroll
-  for (int k = 0; k < 12; ++k) {
-    o[2 * k] = A.b * acc.v[k / 3][k % 3].re;
-    o[2 * k + 1] = A.b * acc.v[k / 3][k % 3].im;
-  }
-  if (A.self) {
-    double x[24];
-    ld_site_part<W, 0, 24>(A.self + field + flat * 24, x);
-#pragma unroll
-    for (int k = 0; k < 24; ++k) o[k] = fma(A.a, x[k], o[k]);
-  }
-  double* dst = A.out + field + flat * 24;
-#pragma unroll
-  for (int k = 0; k < 24; k += W) st_vec<W>(dst + k, o + k);
-}
 
 // ---------------------------------------------------------------- two threads per site
 // Thread j (j = lane & 1) of a pair forms half-spinor row j of every hop (as
@@ -180,8 +76,9 @@ __global__ void __launch_bounds__(kRefSiteBlock, WL_REFSITE_MINB) ref_site_kerne
 // with c' = -i c.  In the reference layout spin s is reals [6s, 6s+6): one
 // 32-byte vector plus one 16-byte half.  The pair's 16-byte halves of spins
 // (0, 1) and of spins (2, 3) share a sector and are requested by the same
-// instruction, so a pair requests every sector of a neighbour's spinor exactly
-// once.  Both threads read the same link addresses in the same instruction.
+// instruction (the load offsets depend on the spin's parity arithmetically, so
+// the pair does not diverge), so a pair requests every sector of a neighbour's
+// spinor exactly once.  Both threads read the same link addresses in the same instruction.
 // Thread j keeps its upper spin A = a_j and partial sums X of a_{3-j} and Y of
 // a_{2+j} (18 doubles instead of 24); at the end two xor-shuffle rounds give
 // thread 0 spins (0, 1) and thread 1 spins (2, 3), and each stores its half of
@@ -192,17 +89,20 @@ template <int W>
 WL_D void ld_spin(const double* site, int s, double (&v)[6]) {
   const double* p = site + 6 * s;
   if (W == 4) {
-    if (s & 1) {  // reals [6s, 6s+2) are the upper half of a 32-byte vector, [6s+2, 6s+6) a whole one
-      const double2 q = __ldg(reinterpret_cast<const double2*>(p));
-      v[0] = q.x;
-      v[1] = q.y;
-      ld_vec<4>(p + 2, v + 2);
-    } else {  // [6s, 6s+4) whole, [6s+4, 6s+6) the lower half of the next
-      ld_vec<4>(p, v);
-      const double2 q = __ldg(reinterpret_cast<const double2*>(p + 4));
-      v[4] = q.x;
-      v[5] = q.y;
-    }
+    // Even s: reals [6s, 6s+4) are a whole 32-byte vector and [6s+4, 6s+6) the lower half of the
+    // next; odd s: [6s, 6s+2) the upper half of a vector and [6s+2, 6s+6) a whole one.  The two
+    // threads of a pair have spins of different parity, so the offsets are computed, not branched
+    // on: both threads issue the same two load instructions.
+    const int odd = s & 1;
+    double q[4], h[2];
+    ld_vec<4>(p + 2 * odd, q);
+    ld_vec<2>(p + 4 - 4 * odd, h);
+    v[0] = odd ? h[0] : q[0];
+    v[1] = odd ? h[1] : q[1];
+    v[2] = odd ? q[0] : q[2];
+    v[3] = odd ? q[1] : q[3];
+    v[4] = odd ? q[2] : h[0];
+    v[5] = odd ? q[3] : h[1];
   } else {
 #pragma unroll
     for (int k = 0; k < 6; k += 2) ld_vec<2>(p + k, v + k);
