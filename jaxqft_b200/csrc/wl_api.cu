@@ -22,7 +22,7 @@
 #include "wl_force.cuh"
 #include "wl_gauge.cuh"
 #include "wl_meas.cuh"
-#include "wl_refsite.cuh"
+#include "wl_reftile.cuh"
 #include "wl_rng.cuh"
 #include "wl_blas.cuh"
 #include "wl_rowhop.cuh"
@@ -573,16 +573,17 @@ static wl_status ensure_tmp(wl_ctx* ctx, size_t bytes) {
   return WL_OK;
 }
 
-// Kernel for the reference-layout hop: 0 = ref_pair_kernel (two threads per
-// site, 256-bit spinor accesses, parity-split SoA links; the default),
-// 1 = row_hop_kernel (TMA row staging), 2 = hop_kernel on the reference layout.
-// WL_REF_HOP=pair|row|generic selects one (for comparisons).
+// Kernel for the reference-layout hop: 0 = ref_tile_kernel where it applies (all sites
+// targeted, Lt a multiple of 16, 32-byte aligned fields), else ref_pair_kernel; 3 =
+// ref_pair_kernel always; 1 = row_hop_kernel (TMA row staging); 2 = hop_kernel on the
+// reference layout.  WL_REF_HOP=tile|pair|row|generic selects one (for comparisons).
 static int ref_hop_kind() {
   static const int k = [] {
     const char* e = std::getenv("WL_REF_HOP");
     if (!e) return 0;
     if (std::strcmp(e, "row") == 0) return 1;
     if (std::strcmp(e, "generic") == 0) return 2;
+    if (std::strcmp(e, "pair") == 0) return 3;
     return 0;
   }();
   return k;
@@ -604,6 +605,20 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
+// The spinor field `in` (nrhs fields) as 128-byte lines of 16 doubles for 2D tensor-map copies
+// with the 128-byte swizzle, `box_lines` lines per copy.  False if the map cannot be built.
+static bool encode_psi_lines_map(const void* in, long long lines, unsigned box_lines, CUtensorMap* map) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || lines >= (1LL << 31) || ((uintptr_t)in & 15) || box_lines == 0 || box_lines > 256) return false;
+  const cuuint64_t dims[2] = {16, (cuuint64_t)lines};
+  const cuuint64_t strides[1] = {128};
+  const cuuint32_t box[2] = {16, box_lines};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(in), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Row-staged (TMA) FP64 hop for the reference layout; false if the lattice does
 // not fit its shared-memory stages or the tensor map cannot be built.
 template <bool DAG>
@@ -613,17 +628,8 @@ static bool row_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const v
   const int Lt = g.L[3];
   if (!row_hop_enabled() || Lt > kRowMaxLt) return false;
   const long long lines = (long long)nrhs * g.V * 3 / 2;  // the fields as 128-byte lines
-  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc || lines >= (1LL << 31) || ((uintptr_t)in & 15)) return false;
   CUtensorMap map;
-  const cuuint64_t dims[2] = {16, (cuuint64_t)lines};
-  const cuuint64_t strides[1] = {128};
-  const cuuint32_t box[2] = {16, (cuuint32_t)(Lt * 3 / 2)};
-  const cuuint32_t estr[2] = {1, 1};
-  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(in), dims, strides, box, estr,
-          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-    return false;
+  if (!encode_psi_lines_map(in, lines, (unsigned)(Lt * 3 / 2), &map)) return false;
   RowHopArgs A{};
   A.g = g;
   A.U = G->ref_copy;
@@ -652,12 +658,40 @@ static bool row_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const v
   return true;
 }
 
+// Warp-tile TMA hop (wl_reftile.cuh): every site targeted, Lt a multiple of 16.
+template <bool DAG>
+static bool tile_hop_launch(wl_ctx* ctx, const RefSiteArgs& A) {
+  const Geom& g = ctx->g;
+  if (g.L[3] % kTileSites != 0) return false;
+  const long long lines = (long long)A.nrhs * g.V * 3 / 2;
+  if (lines >= (1LL << 31) || ((uintptr_t)A.in & 15)) return false;
+  CUtensorMap map;
+  if (!encode_psi_lines_map(A.in, lines, kTileSites * 3 / 2, &map)) return false;
+  const size_t smem = tile_smem_bytes();
+  int per_sm = 0;
+  if (cudaFuncSetAttribute(ref_tile_kernel<DAG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ref_tile_kernel<DAG>, 32 * kTileWarps, smem) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();  // fall back to the pair kernel; clear the error this left
+    return false;
+  }
+  const long long tiles = (long long)(g.V / kTileSites) * A.nrhs;
+  const long long want = (tiles + kTileWarps - 1) / kTileWarps;
+  const int blocks = (int)std::min<long long>(want, (long long)per_sm * ctx->sm_count);
+  g_launches++;
+  ref_tile_kernel<DAG><<<blocks, 32 * kTileWarps, smem, ctx->stream>>>(map, A, ctx->dev_err);
+  return true;
+}
+
 // Site-parallel reference-layout hop (wl_refsite.cuh); parity < 0 targets every site.
 template <bool DAG>
 static bool site_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const void* self, double a, double b,
                      int nrhs, int parity) {
   const Geom& g = ctx->g;
-  if (ref_hop_kind() != 0 || nrhs > 65535) return false;
+  const int kind = ref_hop_kind();
+  if ((kind != 0 && kind != 3) || nrhs > 65535) return false;
   RefSiteArgs A{};
   A.g = g;
   A.U = G->d18;
@@ -668,9 +702,10 @@ static bool site_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const 
   A.b = b;
   A.nrhs = nrhs;
   A.parity = parity;
+  const bool w32 = (((uintptr_t)in | (uintptr_t)out | (uintptr_t)self) & 31) == 0;
+  if (kind == 0 && parity < 0 && w32 && tile_hop_launch<DAG>(ctx, A)) return true;
   const long long n = (parity < 0 ? g.V : g.Vh) * 2LL;  // two threads per target site
   const dim3 grid((unsigned)((n + kRefSiteBlock - 1) / kRefSiteBlock), nrhs);
-  const bool w32 = (((uintptr_t)in | (uintptr_t)out | (uintptr_t)self) & 31) == 0;
   g_launches++;
   if (w32) ref_pair_kernel<DAG, 4><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
   else ref_pair_kernel<DAG, 2><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);

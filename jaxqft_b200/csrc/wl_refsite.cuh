@@ -109,19 +109,20 @@ WL_D void ld_spin(const double* site, int s, double (&v)[6]) {
   }
 }
 
-template <int MU, int C, int W>
-WL_D void refpair_project(const double* site, int j, double sg, cplx<double> (&h)[3]) {
-  const int s1 = (MU == 3 && C < 0) ? 2 + j : j;
-  double a[6];
-  ld_spin<W>(site, s1, a);
+// the two spins thread j of a pair projects from: s1 (always) and s2 (mu < 3)
+template <int MU, int C>
+WL_D int pair_spin1(int j) { return (MU == 3 && C < 0) ? 2 + j : j; }
+template <int MU>
+WL_D int pair_spin2(int j) { return MU == 2 ? 2 + j : 3 - j; }
+
+// half-spinor row j of (1 + C g_mu) psi from its spins a = s1, b = s2 (6 reals each)
+template <int MU, int C>
+WL_D void pair_combine(const double (&a)[6], const double (&b)[6], double sg, cplx<double> (&h)[3]) {
   if (MU == 3) {
 #pragma unroll
     for (int col = 0; col < 3; ++col) h[col] = {2.0 * a[2 * col], 2.0 * a[2 * col + 1]};
     return;
   }
-  const int s2 = MU == 2 ? 2 + j : 3 - j;
-  double b[6];
-  ld_spin<W>(site, s2, b);
 #pragma unroll
   for (int col = 0; col < 3; ++col) {
     const cplx<double> av{a[2 * col], a[2 * col + 1]}, bv{b[2 * col], b[2 * col + 1]};
@@ -133,6 +134,81 @@ WL_D void refpair_project(const double* site, int j, double sg, cplx<double> (&h
       else h[col] = av + w;
     }
   }
+}
+
+template <int MU, int C, int W>
+WL_D void refpair_project(const double* site, int j, double sg, cplx<double> (&h)[3]) {
+  double a[6], b[6];
+  ld_spin<W>(site, pair_spin1<MU, C>(j), a);
+  if (MU < 3) ld_spin<W>(site, pair_spin2<MU>(j), b);
+  pair_combine<MU, C>(a, b, sg, h);
+}
+
+// links of one hop: forward U_mu(x) (stored with the target's parity p, compact c) or
+// backward U_mu(x - mu) (parity 1 - p, compact index of the neighbour)
+WL_D void ld_link(const double2* U, unsigned vh, int p, int mu, int c, Link<double>& u) {
+  const double2* lk = U + (size_t)(p * 4 + mu) * 9 * vh + c;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const double2 q = ldg(lk + (size_t)k * vh);
+    u.m[k / 3][k % 3] = {q.x, q.y};
+  }
+}
+
+// the pair's epilogue: assemble spins (0,1) in thread 0 and (2,3) in thread 1
+// (a0 = A_0, a1 = A_1, a2 = Y_0 + X_1, a3 = X_0 + Y_1, subscript = thread of the pair:
+// round 1 thread 0 sends X_0 and receives A_1, round 2 thread 0 sends Y_0), then
+// out = a*self + b*acc for this thread's two spins.  Every lane must call it.
+template <int W>
+WL_D void pair_store(const RefSiteArgs& A, size_t off, bool act, int j, const cplx<double> (&Ac)[3],
+                     const cplx<double> (&Xc)[3], const cplx<double> (&Yc)[3]) {
+  cplx<double> lo[3], hi[3];  // thread 0: spins 0, 1; thread 1: spins 2, 3
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const cplx<double> r1 = shfl_pair(j == 0 ? Xc[a] : Ac[a]);
+    const cplx<double> r2 = shfl_pair(Yc[a]);
+    if (j == 0) {
+      lo[a] = Ac[a];
+      hi[a] = r1;
+    } else {
+      lo[a] = r2 + Xc[a];
+      hi[a] = r1 + Yc[a];
+    }
+  }
+  if (!act) return;
+  double o[12];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    o[2 * a] = A.b * lo[a].re;
+    o[2 * a + 1] = A.b * lo[a].im;
+    o[6 + 2 * a] = A.b * hi[a].re;
+    o[6 + 2 * a + 1] = A.b * hi[a].im;
+  }
+  if (A.self) {
+    double x[12];
+#pragma unroll
+    for (int k = 0; k < 12; k += W) ld_vec<W>(A.self + off + k, x + k);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) o[k] = fma(A.a, x[k], o[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < 12; k += W) st_vec<W>(A.out + off + k, o + k);
+}
+
+// site coordinates of flat index f
+WL_D Site site_of_flat(const Geom& g, int f) {
+  Site s;
+  const int c = f >> 1;
+  const int row = (int)fdiv(g.fd_lth, (unsigned)c);
+  const int t = f - row * g.L[3];
+  const int r2 = (int)fdiv(g.fd_l2, (unsigned)row);
+  s.c = WL_CHECKED(c, g.Vh);
+  s.row = row;
+  s.x[2] = row - r2 * g.L[2];
+  s.x[0] = (int)fdiv(g.fd_l1, (unsigned)r2);
+  s.x[1] = r2 - s.x[0] * g.L[1];
+  s.x[3] = t;
+  return s;
 }
 
 template <int MU, bool DAG, int W>
@@ -148,14 +224,9 @@ WL_D void refpair_mu(const RefSiteArgs& A, const double* base, const Site& s, in
     int tn = s.x[3];
     if (MU == 3) tn = dir == 0 ? (tn == g.L[3] - 1 ? 0 : tn + 1) : (tn == 0 ? g.L[3] - 1 : tn - 1);
     const double* src = base + (size_t)(2 * nb + (tn & 1)) * 24;
-    const double2* lk = dir == 0 ? A.U + (size_t)(parity * 4 + MU) * 9 * vh + s.c
-                                 : A.U + (size_t)((1 - parity) * 4 + MU) * 9 * vh + nb;
     Link<double> u;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      const double2 q = ldg(lk + (size_t)k * vh);
-      u.m[k / 3][k % 3] = {q.x, q.y};
-    }
+    if (dir == 0) ld_link(A.U, vh, parity, MU, s.c, u);
+    else ld_link(A.U, vh, 1 - parity, MU, nb, u);
     cplx<double> h[3];
     if (dir == 0) {
       refpair_project<MU, CF, W>(src, j, sg, h);
@@ -187,17 +258,8 @@ __global__ void __launch_bounds__(kRefSiteBlock, WL_REFPAIR_MINB) ref_pair_kerne
   const size_t field = (size_t)rhs * g.V * 24;
   if (act) {
     if (A.parity < 0) {  // every site: i is the flat index
-      const int c = i >> 1;
-      const int row = (int)fdiv(g.fd_lth, (unsigned)c);
-      const int t = i - row * g.L[3];
-      const int r2 = (int)fdiv(g.fd_l2, (unsigned)row);
-      s.c = WL_CHECKED(c, g.Vh);
-      s.row = row;
-      s.x[2] = row - r2 * g.L[2];
-      s.x[0] = (int)fdiv(g.fd_l1, (unsigned)r2);
-      s.x[1] = r2 - s.x[0] * g.L[1];
-      s.x[3] = t;
-      parity = (s.x[0] + s.x[1] + s.x[2] + t) & 1;
+      s = site_of_flat(g, i);
+      parity = (s.x[0] + s.x[1] + s.x[2] + s.x[3]) & 1;
     } else {  // one parity: i is the compact index
       parity = A.parity;
       s = site_from_compact(g, parity, i);
@@ -208,41 +270,8 @@ __global__ void __launch_bounds__(kRefSiteBlock, WL_REFPAIR_MINB) ref_pair_kerne
     refpair_mu<2, DAG, W>(A, base, s, parity, j, sg, Ac, Xc, Yc);
     refpair_mu<3, DAG, W>(A, base, s, parity, j, sg, Ac, Xc, Yc);
   }
-  // a0 = A_0, a1 = A_1, a2 = Y_0 + X_1, a3 = X_0 + Y_1 (subscript = thread of the pair).
-  // Round 1: thread 0 sends X_0 and receives A_1; round 2: thread 0 sends Y_0.
-  cplx<double> lo[3], hi[3];  // thread 0: spins 0, 1; thread 1: spins 2, 3
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const cplx<double> r1 = shfl_pair(j == 0 ? Xc[a] : Ac[a]);
-    const cplx<double> r2 = shfl_pair(Yc[a]);
-    if (j == 0) {
-      lo[a] = Ac[a];
-      hi[a] = r1;
-    } else {
-      lo[a] = r2 + Xc[a];  // a2 = Y_0 + X_1
-      hi[a] = r1 + Yc[a];  // a3 = X_0 + Y_1
-    }
-  }
-  if (!act) return;
   const size_t flat = (size_t)s.row * g.L[3] + s.x[3];
-  double o[12];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    o[2 * a] = A.b * lo[a].re;
-    o[2 * a + 1] = A.b * lo[a].im;
-    o[6 + 2 * a] = A.b * hi[a].re;
-    o[6 + 2 * a + 1] = A.b * hi[a].im;
-  }
-  const size_t off = field + flat * 24 + 12 * j;  // this thread's two spins
-  if (A.self) {
-    double x[12];
-#pragma unroll
-    for (int k = 0; k < 12; k += W) ld_vec<W>(A.self + off + k, x + k);
-#pragma unroll
-    for (int k = 0; k < 12; ++k) o[k] = fma(A.a, x[k], o[k]);
-  }
-#pragma unroll
-  for (int k = 0; k < 12; k += W) st_vec<W>(A.out + off + k, o + k);
+  pair_store<W>(A, field + flat * 24 + 12 * j, act, j, Ac, Xc, Yc);  // this thread's two spins
 }
 
 }  // namespace wl
