@@ -416,7 +416,7 @@ def run_serving(args, dev):
     from jaxqft_b200.serving import PropagatorServer, serve_once, warm_server
 
     server = PropagatorServer(SERVE_VOLUMES, gauge_seeds=(0, 1, 2, 3), nslots=16, inner="half", tol=TOL,
-                              device=dev)
+                              device=dev, keep_solutions=False)
     warm_server(server)  # every engine allocated, tuned and graph-captured before the timed streams
     out = serve_once(server, args.serve_rate, args.serve_seconds)
     out.update({"volumes": ["x".join(map(str, v)) for v in SERVE_VOLUMES], "gauge_fields_per_volume": 4,

@@ -115,12 +115,16 @@ class PropagatorServer:
     def __init__(self, volumes: Sequence[Tuple[int, ...]], gauge_seeds: Sequence[int] = (0, 1, 2, 3),
                  link_scale: float = 0.2, nslots: int = 16, inner: str = "half", tol: float = 1e-10,
                  maxiter: int = 4000, hbm_budget_bytes: Optional[int] = None, iters_per_poll: int = 8,
-                 device=None):
+                 device=None, keep_solutions: bool = True):
         if not torch.cuda.is_available():
             raise RuntimeError("the serving loop requires a CUDA device")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.nslots, self.inner, self.tol, self.maxiter = int(nslots), inner, float(tol), int(maxiter)
         self.iters_per_poll = int(iters_per_poll)
+        # False: a finished request's device buffers (sources, right-hand sides, solutions) are
+        # released as soon as it completes, as a server does once the response has been sent;
+        # only its statistics (and its pion correlator) are kept
+        self.keep_solutions = bool(keep_solutions)
         free, total = torch.cuda.mem_get_info(self.device)
         self.hbm_budget = int(hbm_budget_bytes) if hbm_budget_bytes is not None else int(0.6 * free)
         self.ctx: Dict[Tuple[int, ...], L.WilsonContext] = {}
@@ -249,6 +253,8 @@ class PropagatorServer:
                             if req.measure == "pion":
                                 self._measure_pion(req)
                             req.t_done = time_fn() - t0
+                            if not self.keep_solutions:
+                                req.eta = req.b = req.x = None
                             self.done.append(req)
             if now >= next_sample:
                 self.trace.append((now, len(self.queue), sum(len(e.owner) for e in self.engines.values())))
@@ -367,7 +373,7 @@ def main(argv=None):
     ap.add_argument("--seconds", type=float, default=30.0, help="arrival window per rate")
     ap.add_argument("--inner", default="half")
     args = ap.parse_args(argv)
-    server = PropagatorServer(VOLUMES, gauge_seeds=(0, 1, 2, 3), nslots=16, inner=args.inner)
+    server = PropagatorServer(VOLUMES, gauge_seeds=(0, 1, 2, 3), nslots=16, inner=args.inner, keep_solutions=False)
     warm_server(server)
     for rate in (float(r) for r in args.rates.split(",")):
         s = serve_once(server, rate, args.seconds)

@@ -600,12 +600,19 @@ class SU3WilsonNf2(SU3YangMills):
         tol = self.cg_tol if tol is None else float(tol)
         x = solve_normal_eq(b)
         bn = torch.stack([_field_norm(b[i]) for i in range(b.shape[0])])
+        shape = (b.shape[0],) + (1,) * (b.dim() - 1)
         for _ in range(int(self.max_refine_rounds)):
             r = b - apply_A(x)
             rn = torch.stack([_field_norm(r[i]) for i in range(r.shape[0])])
-            if bool(torch.all(rn <= tol * bn)):
+            done = rn <= tol * bn
+            if bool(torch.all(done)):
                 return x
-            x = x + solve_normal_eq(r)
+            # each correction is solved for the residual scaled to unit norm (entries that already
+            # meet the rule get a zero right-hand side), so that the reduced-precision iterations
+            # see O(1) values however small the residual has become
+            scale = torch.where(done, torch.zeros_like(rn), rn)
+            inv = torch.where(done, torch.zeros_like(rn), 1.0 / torch.where(done, torch.ones_like(rn), rn))
+            x = x + scale.reshape(shape).to(x.dtype) * solve_normal_eq(r * inv.reshape(shape).to(r.dtype))
         warnings.warn(f"direct residual did not reach tol {tol} in {self.max_refine_rounds} refinements",
                       RuntimeWarning)
         return x

@@ -113,6 +113,7 @@ def make_server(volumes, nslots, budget, engine_bytes):
     srv = object.__new__(serving.PropagatorServer)
     srv.device = torch.device("cpu")
     srv.nslots, srv.inner, srv.tol, srv.maxiter, srv.iters_per_poll = nslots, "half", 1e-10, 100, 8
+    srv.keep_solutions = True
     srv.hbm_budget = budget
     srv.ctx = {v: FakeCtx(v, engine_bytes) for v in volumes}
     srv.gauges = {(v, s): object() for v in volumes for s in range(2)}
@@ -179,6 +180,16 @@ def test_serving_trace_and_queue_summary(fake_engines):
     q = serving.queue_summary(srv.trace, arrival_window=0.0, points=5)
     assert q["max_queued"] >= 1 and len(q["samples"]) <= 5
     assert serving.queue_summary([], 1.0)["max_queued"] == 0
+
+
+def test_serving_releases_finished_requests_buffers(fake_engines):
+    srv = make_server([VOL], nslots=8, budget=10**9, engine_bytes=100)
+    srv.keep_solutions = False
+    reqs = [serving.Request(rid=i, volume=VOL, gauge=0, kappa=0.125, nrhs=2, kind="point", t_arrive=0.0)
+            for i in range(3)]
+    done = srv.run(reqs, time_fn=FakeClock(1e-3))
+    assert len(done) == 3 and all(r.x is None and r.b is None and r.eta is None for r in done)
+    assert all(len(r.stats) == 2 for r in done)
 
 
 def test_serving_waits_for_free_slots(fake_engines):
