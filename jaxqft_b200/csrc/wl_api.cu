@@ -217,12 +217,13 @@ struct Tune {
   int nr = 1, bx = 128, by = 1;
   int lanes = 0;  // > 0: RHS-in-lanes hop (FP16/FP32 storage) with this many RHS lanes per site
   int pair = 0;   // 1: FP64 single-RHS stencil with two threads per site (hop_pair_kernel)
+  int seq = 1;    // FP64 RHS-in-lanes hop: groups of `lanes` RHS each block works through in turn
 };
 
 static dim3 grid_for(const Geom& g, const Tune& t, int nrhs, int npar) {
   if (t.lanes > 0) {
-    const int S = kLaneBlock / t.lanes;
-    return dim3((g.Vh + S - 1) / S, (nrhs + t.lanes - 1) / t.lanes, npar);
+    const int S = kLaneBlock / t.lanes, per = t.lanes * std::max(1, t.seq);
+    return dim3((g.Vh + S - 1) / S, (nrhs + per - 1) / per, npar);
   }
   if (t.pair) return dim3((g.Vh + t.bx / 2 - 1) / (t.bx / 2), nrhs, npar);
   int groups = (nrhs + t.nr - 1) / t.nr;
@@ -269,9 +270,12 @@ static void launch_hop_impl(const Tune& t, const HopArgs<LF, SF, EPI>& a, int np
   if constexpr (std::is_same<SF, SpinorField<P_DOUBLE>>::value && std::is_same<IDX, IdxCompact>::value) {
     if (t.lanes > 0) {  // FP64 fields stored RHS-innermost
       dim3 lb(kLaneBlock, 1, 1);
-      switch (t.lanes) {
-        case 16: hop_lanes_d_kernel<DAG, 16><<<grid, lb, 0, st>>>(a); break;
-        case 8: hop_lanes_d_kernel<DAG, 8><<<grid, lb, 0, st>>>(a); break;
+      switch (t.lanes * 10 + t.seq) {
+        case 161: hop_lanes_d_kernel<DAG, 16><<<grid, lb, 0, st>>>(a); break;
+        case 81: hop_lanes_d_kernel<DAG, 8><<<grid, lb, 0, st>>>(a); break;
+        case 82: hop_lanes_d_kernel<DAG, 8, LF, EPI, 2><<<grid, lb, 0, st>>>(a); break;
+        case 42: hop_lanes_d_kernel<DAG, 4, LF, EPI, 2><<<grid, lb, 0, st>>>(a); break;
+        case 44: hop_lanes_d_kernel<DAG, 4, LF, EPI, 4><<<grid, lb, 0, st>>>(a); break;
         default: hop_lanes_d_kernel<DAG, 4><<<grid, lb, 0, st>>>(a); break;
       }
       return;
@@ -1653,11 +1657,14 @@ static Tune pick_update_tune(wl_engine* E, cudaStream_t st) {
   Tune t;
   t.bx = kLaneBlock;
   t.lanes = n > 8 ? 16 : (n > 4 ? 8 : 4);
-  // WL_FORCE_UPDATE_TUNE="lanes" pins the shape
+  // WL_FORCE_UPDATE_TUNE="lanes[,seq]" pins the shape
   if (const char* f = std::getenv("WL_FORCE_UPDATE_TUNE")) {
-    int lanes = 0;
-    if (std::sscanf(f, "%d", &lanes) == 1 && (lanes == 4 || lanes == 8 || lanes == 16)) {
+    int lanes = 0, seq = 1;
+    const int got = std::sscanf(f, "%d,%d", &lanes, &seq);
+    const bool ok_seq = seq == 1 || (lanes == 8 && seq == 2) || (lanes == 4 && (seq == 2 || seq == 4));
+    if (got >= 1 && (lanes == 4 || lanes == 8 || lanes == 16) && ok_seq) {
       t.lanes = lanes;
+      t.seq = seq;
       return t;
     }
   }
@@ -1672,10 +1679,13 @@ static Tune pick_update_tune(wl_engine* E, cudaStream_t st) {
     const int reps = E->ctx->g.Vh >= 65536 ? 3 : 10;
     float best_ms = 1e30f;
     Tune best = t;
-    for (int lanes : {4, 8, 16}) {
-      if (lanes > n && lanes > 4) continue;
+    const int shapes[][2] = {{4, 1}, {4, 2}, {4, 4}, {8, 1}, {8, 2}, {16, 1}};
+    for (const auto& sh : shapes) {
+      const int lanes = sh[0], seq = sh[1];
+      if ((lanes > n && lanes > 4) || (seq > 1 && lanes * seq > n)) continue;
       Tune c = t;
       c.lanes = lanes;
+      c.seq = seq;
       for (int trial = 0; trial < 3; ++trial) {
         const float ms = time_update_hop(E, st, c, reps);
         if (cudaGetLastError() == cudaSuccess && ms < best_ms) {
@@ -1688,8 +1698,8 @@ static Tune pick_update_tune(wl_engine* E, cudaStream_t st) {
   }
   const char* verb = std::getenv("WL_VERBOSE");
   if (verb && verb[0] == '1')
-    std::fprintf(stderr, "[wl] update tune vh=%d links12=%d nslots=%d op=%d -> lanes=%d\n", k.vh,
-                 (int)E->ru_links12, n, k.op, t.lanes);
+    std::fprintf(stderr, "[wl] update tune vh=%d links12=%d nslots=%d op=%d -> lanes=%d seq=%d\n", k.vh,
+                 (int)E->ru_links12, n, k.op, t.lanes, t.seq);
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune_cache[k] = t;
   return t;

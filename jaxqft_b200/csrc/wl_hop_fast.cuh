@@ -410,19 +410,23 @@ WL_D void lane_dir(const SF& src, const LinkSmem* Ls, const int* nbs, int rhs, f
 constexpr int kLaneWarps = kLaneBlock / 32;
 static_assert(kLaneWarps == 4, "reduce_lanes adds four warps");
 
+// rbase: first RHS of the block's group (blockIdx.y * R unless a block works through several
+// groups); a block that calls it more than once must pass again = true after the first call.
 template <int R>
-WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* /*mask*/) {
+WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* /*mask*/, int rbase = -1,
+                       bool again = false) {
   __shared__ double sred[kLaneWarps][32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 #pragma unroll
   for (int off = R; off < 32; off <<= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if (again) __syncthreads();  // the previous call's readers are done with sred
   if (lane < R) sred[warp][lane] = v;
   __syncthreads();
   if (tid < R) {
     const double x = (sred[0][tid] + sred[1][tid]) + (sred[2][tid] + sred[3][tid]);
     const int nblk = gridDim.x * gridDim.z;
     const int blk = blockIdx.z * gridDim.x + blockIdx.x;
-    const int rhs = blockIdx.y * R + tid;
+    const int rhs = (rbase < 0 ? (int)blockIdx.y * R : rbase) + tid;
     if (rhs < nrhs) Rd.partials[(long long)rhs * nblk + blk] = x;
   }
 }
@@ -595,7 +599,10 @@ WL_D void lane_dir_d(const SpinorField<P_DOUBLE>& src, const SiteLinksD& Ls, con
   }
 }
 
-template <bool DAG, int R, class LF, class EPI>
+// G > 1: the block works through G groups of R right-hand sides one after the other on the
+// links it staged once (grid.y = ceil(nrhs / (R G))), so each link is read once per launch
+// instead of once per group.
+template <bool DAG, int R, class LF, class EPI, int G = 1>
 __global__ void __launch_bounds__(kLaneBlock, WL_LANE_D_MIN_BLOCKS) hop_lanes_d_kernel(HopArgs<LF, SpinorField<P_DOUBLE>, EPI> A) {
   constexpr int S = kLaneBlock / R;
   __shared__ LaneSmemD<R> sm;
@@ -633,20 +640,24 @@ __global__ void __launch_bounds__(kLaneBlock, WL_LANE_D_MIN_BLOCKS) hop_lanes_d_
   }
   __syncwarp();
   const int sl = tid / R;
-  const int rhs = blockIdx.y * R + (tid % R);
-  double red = 0.0;
-  const bool act = sm.ok[sl] && rhs < A.nrhs && (A.mask == nullptr || A.mask[rhs] != 0);
-  if (act) {
-    Spinor<double> acc;
-    zero(acc);
-    const SpinorField<P_DOUBLE>& src = A.src[1 - parity];
-    lane_dir_d<0, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
-    lane_dir_d<1, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
-    lane_dir_d<2, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
-    lane_dir_d<3, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
-    red = A.epi(rhs, parity, (long long)sm.c[sl], acc);
+#pragma unroll 1
+  for (int u = 0; u < G; ++u) {
+    const int rbase = ((int)blockIdx.y * G + u) * R;
+    const int rhs = rbase + (tid % R);
+    double red = 0.0;
+    const bool act = sm.ok[sl] && rhs < A.nrhs && (A.mask == nullptr || A.mask[rhs] != 0);
+    if (act) {
+      Spinor<double> acc;
+      zero(acc);
+      const SpinorField<P_DOUBLE>& src = A.src[1 - parity];
+      lane_dir_d<0, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
+      lane_dir_d<1, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
+      lane_dir_d<2, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
+      lane_dir_d<3, DAG>(src, sm.link[sl], sm.nb[sl], rhs, acc);
+      red = A.epi(rhs, parity, (long long)sm.c[sl], acc);
+    }
+    if (EPI::kReduce) reduce_lanes<R>(red, A.red, A.nrhs, A.mask, rbase, u > 0);
   }
-  if (EPI::kReduce) reduce_lanes<R>(red, A.red, A.nrhs, A.mask);
 }
 
 }  // namespace wl

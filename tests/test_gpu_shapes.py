@@ -131,10 +131,11 @@ def forced_update(request):
     del os.environ["WL_FORCE_UPDATE_TUNE"]
 
 
-@pytest.mark.parametrize("forced_update", ["16", "8", "4"], indirect=True)
+@pytest.mark.parametrize("forced_update", ["16", "8", "4", "8,2", "4,2", "4,4"], indirect=True)
 def test_update_hop_shapes(setup, forced_update):
-    """Every shape of the FP64 reliable-update hop (RHS lanes per sweep) gives solves
-    that reach the FP64 true-residual tolerance, checked against the oracle operator."""
+    """Every shape of the FP64 reliable-update hop (RHS lanes per group, groups a block
+    works through on its staged links) gives solves that reach the FP64 true-residual
+    tolerance, checked against the oracle operator."""
     shape, U, bc, ctx, gauge, rng = setup
     n = 13
     masses = np.linspace(-0.3, 0.1, n)

@@ -33,7 +33,7 @@ def test_tile_kernel_operators(shape, bc, nrhs):
     psi = W.gaussian_spinor(rng, shape, nrhs)
     bc64 = tuple(complex(np.complex64(complex(b))) for b in bc)
     mass = -0.2
-    ctx = WilsonContext(shape, bc=bc)
+    ctx = WilsonContext(shape, bc=bc64)  # phases as the theory layer passes them (rounded through complex64)
     gauge = ctx.gauge(torch.from_numpy(U[0]))
     x = torch.from_numpy(psi).cuda()
     D = ctx.apply("D", gauge, mass, x).cpu().numpy()
