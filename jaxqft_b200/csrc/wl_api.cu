@@ -234,6 +234,16 @@ template <class SF> struct UsesFastHop : std::false_type {};
 template <> struct UsesFastHop<SpinorField<P_SINGLE>> : std::true_type {};
 template <> struct UsesFastHop<SpinorField<P_HALF>> : std::true_type {};
 
+// WL_HALF_COLOR=1: the FP16 RHS-in-lanes hop multiplies by the links in packed FP16 (HFMA2)
+// instead of FP32 pairs (an option for comparisons; off by default)
+static bool half_color_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("WL_HALF_COLOR");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
 static bool fast_hop_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("WL_FAST_HOP");
@@ -286,6 +296,17 @@ static void launch_hop_impl(const Tune& t, const HopArgs<LF, SF, EPI>& a, int np
     }
   }
   if constexpr (UsesFastHop<SF>::value && std::is_same<IDX, IdxCompact>::value) {
+    if constexpr (std::is_same<SF, SpinorField<P_HALF>>::value) {
+      if (t.lanes > 0 && half_color_enabled()) {  // colour multiply in packed FP16 (HFMA2)
+        dim3 lb(kLaneBlock, 1, 1);
+        switch (t.lanes) {
+          case 16: hop_lanes_kernel<DAG, 16, LF, SF, EPI, true><<<grid, lb, 0, st>>>(a); break;
+          case 8: hop_lanes_kernel<DAG, 8, LF, SF, EPI, true><<<grid, lb, 0, st>>>(a); break;
+          default: hop_lanes_kernel<DAG, 4, LF, SF, EPI, true><<<grid, lb, 0, st>>>(a); break;
+        }
+        return;
+      }
+    }
     if (t.lanes > 0) {
       dim3 lb(kLaneBlock, 1, 1);
       switch (t.lanes) {

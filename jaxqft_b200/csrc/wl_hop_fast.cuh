@@ -335,6 +335,42 @@ WL_D void color_mul_smem(const LinkSmem& L, const float2 (&h)[6], float2 (&uh)[6
 
 WL_D __half2 as_h2(unsigned int u) { return *reinterpret_cast<__half2*>(&u); }
 
+// the projection as half2 values (rows 0, 1 x colours), no conversion; returns the site norm
+template <int MU, int C>
+WL_D float load_project_half2(const SpinorField<P_HALF>& f, int rhs, unsigned c, __half2 (&h)[6]) {
+  const float n = ldg(f.norm + f.nat(rhs, c));
+  __half2 s[12];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (MU == 3 && ((C > 0 && k == 2) || (C < 0 && k == 0))) continue;
+    const uint4 v = ldg(f.ptr + f.at(rhs, k, c));
+    s[4 * k + 0] = as_h2(v.x);
+    s[4 * k + 1] = as_h2(v.y);
+    s[4 * k + 2] = as_h2(v.z);
+    s[4 * k + 3] = as_h2(v.w);
+  }
+  const __half2 pcm = __floats2half2_rn((float)C, -(float)C);  // -iC x = pcm * swap(x)
+  const __half2 pmc = __floats2half2_rn(-(float)C, (float)C);  //  iC x = pmc * swap(x)
+#pragma unroll
+  for (int col = 0; col < 3; ++col) {
+    const __half2 s0 = s[col], s1 = s[3 + col], s2 = s[6 + col], s3 = s[9 + col];
+    if (MU == 0) {
+      h[col] = C > 0 ? __hadd2(s0, s3) : __hsub2(s0, s3);
+      h[3 + col] = C > 0 ? __hadd2(s1, s2) : __hsub2(s1, s2);
+    } else if (MU == 1) {
+      h[col] = __hfma2(pcm, __lowhigh2highlow(s3), s0);
+      h[3 + col] = __hfma2(pmc, __lowhigh2highlow(s2), s1);
+    } else if (MU == 2) {
+      h[col] = __hfma2(pcm, __lowhigh2highlow(s2), s0);
+      h[3 + col] = __hfma2(pcm, __lowhigh2highlow(s3), s1);
+    } else {
+      h[col] = C > 0 ? s0 : s2;
+      h[3 + col] = C > 0 ? s1 : s3;
+    }
+  }
+  return n;
+}
+
 template <int MU, int C>
 WL_D float load_project_half(const SpinorField<P_HALF>& f, int rhs, unsigned c, float2 (&h)[6]) {
   const float n = ldg(f.norm + f.nat(rhs, c));
@@ -403,6 +439,61 @@ WL_D void lane_dir(const SF& src, const LinkSmem* Ls, const int* nbs, int rhs, f
   }
 }
 
+// Colour multiply in packed FP16 (HFMA2, FP16 accumulation of the three terms), for the
+// WL_HALF_COLOR variant: the link element k of a hop is staged as two half2, (re, re) and
+// (-im, im) for a forward hop, (re, re) and (im, -im) -- the conjugate -- for a backward one,
+// so U h and U^dag h are the same two HFMA2 per complex multiply-add.  h stays in FP16 (no
+// conversion); the six products are converted to FP32 for the accumulation.
+struct LinkSmemH {
+  uint2 p[9];  // (re, re), (-+im, +-im) as half2 pairs
+};
+
+template <bool DAGU>
+WL_D void color_mul_half(const LinkSmemH& L, const __half2 (&h)[6], float2 (&uh)[6]) {
+#pragma unroll
+  for (int sp = 0; sp < 2; ++sp) {
+    __half2 hs[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) hs[b] = __lowhigh2highlow(h[sp * 3 + b]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      __half2 acc = __float2half2_rn(0.f);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const uint2 q = DAGU ? L.p[b * 3 + a] : L.p[a * 3 + b];
+        acc = __hfma2(as_h2(q.x), h[sp * 3 + b], acc);
+        acc = __hfma2(as_h2(q.y), hs[b], acc);
+      }
+      uh[sp * 3 + a] = __half22float2(acc);
+    }
+  }
+}
+
+// Ls: the site's LinkSmem slots; a hop's FP16 pairs sit at the start of its slot
+template <int MU, bool DAG>
+WL_D void lane_dir_hc(const SpinorField<P_HALF>& src, const LinkSmem* Ls, const int* nbs, int rhs,
+                      float2 (&acc)[12]) {
+  constexpr int CF = DAG ? +1 : -1;
+  constexpr int CB = -CF;
+  constexpr float W3 = (MU == 3) ? 2.0f : 1.0f;
+#pragma unroll
+  for (int dir = 0; dir < 2; ++dir) {
+    const int q = 2 * MU + dir;
+    __half2 h[6];
+    float2 uh[6];
+    const float n = (dir == 0 ? load_project_half2<MU, CF>(src, rhs, (unsigned)nbs[q], h)
+                              : load_project_half2<MU, CB>(src, rhs, (unsigned)nbs[q], h)) * W3;
+    const LinkSmemH& L = *reinterpret_cast<const LinkSmemH*>(&Ls[q]);
+    if (dir == 0) {
+      color_mul_half<false>(L, h, uh);
+      accum2<MU, CF>(acc, uh, n);
+    } else {
+      color_mul_half<true>(L, h, uh);
+      accum2<MU, CB>(acc, uh, n);
+    }
+  }
+}
+
 // Per-block partial sums: xor-shuffles over the sites of a warp leave lanes
 // 0..R-1 with the warp's sum for RHS rbase + lane; after one barrier threads
 // 0..R-1 add the block's warps in a fixed order and block b writes
@@ -431,8 +522,9 @@ WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* /*mask*/
   }
 }
 
-template <bool DAG, int R, class LF, class SF, class EPI>
+template <bool DAG, int R, class LF, class SF, class EPI, bool HC = false>
 __global__ void __launch_bounds__(kLaneBlock, LaneMinBlocks<DAG, EPI>::value) hop_lanes_kernel(HopArgs<LF, SF, EPI> A) {
+  static_assert(!HC || std::is_same<SF, SpinorField<P_HALF>>::value, "FP16 colour multiply needs FP16 fields");
   constexpr int S = kLaneBlock / R;
   __shared__ LaneSmem<R> sm;
   const int tid = threadIdx.x;
@@ -460,10 +552,20 @@ __global__ void __launch_bounds__(kLaneBlock, LaneMinBlocks<DAG, EPI>::value) ho
 #pragma unroll
         for (int k = 0; k < 9; ++k) u.m[k / 3][k % 3] = u.m[k / 3][k % 3] * w;
       }
+      if constexpr (HC) {
+        LinkSmemH* lh = reinterpret_cast<LinkSmemH*>(&sm.link[sl].l[q]);
+        const float sgn = dir == 0 ? 1.0f : -1.0f;  // backward hops use the conjugate
 #pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        const cplx<float> v = u.m[k / 3][k % 3];
-        sm.link[sl].l[q].p[k] = make_float4(v.re, v.re, -v.im, v.im);
+        for (int k = 0; k < 9; ++k) {
+          const cplx<float> v = u.m[k / 3][k % 3];
+          lh->p[k] = make_uint2(f2h(v.re, v.re), f2h(-sgn * v.im, sgn * v.im));
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          const cplx<float> v = u.m[k / 3][k % 3];
+          sm.link[sl].l[q].p[k] = make_float4(v.re, v.re, -v.im, v.im);
+        }
       }
       sm.nb[sl][q] = nb;
       if (q == 0) sm.ok[sl] = 1;
@@ -483,12 +585,20 @@ __global__ void __launch_bounds__(kLaneBlock, LaneMinBlocks<DAG, EPI>::value) ho
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc[k] = f2(0.f, 0.f);
     const SF& src = A.src[1 - parity];
-    const LinkSmem* Ls = sm.link[sl].l;
     const int* nbs = sm.nb[sl];
-    lane_dir<0, DAG>(src, Ls, nbs, rhs, acc);
-    lane_dir<1, DAG>(src, Ls, nbs, rhs, acc);
-    lane_dir<2, DAG>(src, Ls, nbs, rhs, acc);
-    lane_dir<3, DAG>(src, Ls, nbs, rhs, acc);
+    if constexpr (HC) {
+      const LinkSmem* Ls = sm.link[sl].l;
+      lane_dir_hc<0, DAG>(src, Ls, nbs, rhs, acc);
+      lane_dir_hc<1, DAG>(src, Ls, nbs, rhs, acc);
+      lane_dir_hc<2, DAG>(src, Ls, nbs, rhs, acc);
+      lane_dir_hc<3, DAG>(src, Ls, nbs, rhs, acc);
+    } else {
+      const LinkSmem* Ls = sm.link[sl].l;
+      lane_dir<0, DAG>(src, Ls, nbs, rhs, acc);
+      lane_dir<1, DAG>(src, Ls, nbs, rhs, acc);
+      lane_dir<2, DAG>(src, Ls, nbs, rhs, acc);
+      lane_dir<3, DAG>(src, Ls, nbs, rhs, acc);
+    }
     red = A.epi.packed(rhs, parity, (unsigned)c, acc);
   }
   if (EPI::kReduce) reduce_lanes<R>(red, A.red, A.nrhs, A.mask);
