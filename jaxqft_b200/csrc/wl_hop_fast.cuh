@@ -439,8 +439,10 @@ WL_D void lane_dir(const SF& src, const LinkSmem* Ls, const int* nbs, int rhs, f
   }
 }
 
-// Colour multiply in packed FP16 (HFMA2, FP16 accumulation of the three terms), for the
-// WL_HALF_COLOR variant: the link element k of a hop is staged as two half2, (re, re) and
+// Colour multiply in packed FP16 (HFMA2, FP16 accumulation of the three terms), the default
+// for FP16 fields: the FP32 pairs of the multiply are what throttles the FMA pipe of the hop
+// (math-pipe stalls about as frequent as L2-gather stalls), and an HFMA2 does the same two
+// multiply-adds in half the pipe time.  The link element k of a hop is staged as two half2, (re, re) and
 // (-im, im) for a forward hop, (re, re) and (im, -im) -- the conjugate -- for a backward one,
 // so U h and U^dag h are the same two HFMA2 per complex multiply-add.  h stays in FP16 (no
 // conversion); the six products are converted to FP32 for the accumulation.

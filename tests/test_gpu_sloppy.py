@@ -151,3 +151,31 @@ def _phase_ctx(shape, U):
     bc = (1, 1, complex(np.cos(np.pi / 3), np.sin(np.pi / 3)), -1)
     ctx = WilsonContext(shape, bc=bc)
     return [(ctx, ctx.gauge(torch.from_numpy(U[0])), bc)]
+
+
+def test_fp16_hop_with_fp32_colour_multiply():
+    """The FP16 engines multiply by the links in packed FP16 by default; the FP32-pair colour
+    multiply (WL_HALF_COLOR=0, kept for comparisons; the choice is read once per process)
+    must meet the same FP16 bounds, checked in a child process."""
+    import os
+    import subprocess
+    import sys
+
+    from tests.conftest import ROOT
+
+    code = ("import tests.test_gpu_sloppy as T, numpy as np, torch\n"
+            "from oracle import wilson as W\n"
+            "shape = (4, 4, 4, 8); rng = np.random.default_rng(7); U = W.hot_links(rng, shape, 1, 0.2)\n"
+            "ctx = T.WilsonContext(shape, bc=(1, 1, 1, -1)); g = ctx.gauge(torch.from_numpy(U[0]))\n"
+            "m = -0.2962963; eng = T.Engine(ctx, g, 1, op='eo_normal', inner='half')\n"
+            "for src, x in T._fields(shape, 1).items():\n"
+            "    xe = W.project(x[None], 0)\n"
+            "    ref = W.schur_even(U, W.schur_even(U, xe, m, (1, 1, 1, -1), normalized=True), m, (1, 1, 1, -1),"
+            " normalized=True, dag=True)\n"
+            "    out = eng.debug_apply(2, m, torch.from_numpy(xe[0])).cpu().numpy()\n"
+            "    assert T.rel(out, ref[0]) < T.TOLS['half'], (src, T.rel(out, ref[0]))\n"
+            "print('fp32 colour ok')\n")
+    env = dict(os.environ, WL_HALF_COLOR="0")
+    res = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True,
+                         timeout=600)
+    assert res.returncode == 0 and "fp32 colour ok" in res.stdout, res.stdout[-2000:] + res.stderr[-4000:]
