@@ -19,7 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwilson_sm100.so")
 SOURCES = ["wl_api.cu"]
 HEADERS = ["wl_common.cuh", "wl_hop.cuh", "wl_hop_fast.cuh", "wl_site.cuh", "wl_force.cuh", "wl_gauge.cuh",
-           "wl_meas.cuh", "wl_rowhop.cuh", "wl_refsite.cuh", "wl_reftile.cuh", "wl_rng.cuh", "wl_blas.cuh"]
+           "wl_meas.cuh", "wl_rowhop.cuh", "wl_refsite.cuh", "wl_reftile.cuh", "wl_rng.cuh", "wl_blas.cuh",
+           "wl_hop_mma.cuh"]
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC_FLAGS = [

@@ -28,6 +28,7 @@
 #include "wl_rowhop.cuh"
 #include "wl_hop_fast.cuh"
 #include "wl_site.cuh"
+#include "wl_hop_mma.cuh"
 
 using namespace wl;
 
@@ -218,9 +219,15 @@ struct Tune {
   int lanes = 0;  // > 0: RHS-in-lanes hop (FP16/FP32 storage) with this many RHS lanes per site
   int pair = 0;   // 1: FP64 single-RHS stencil with two threads per site (hop_pair_kernel)
   int seq = 1;    // FP64 RHS-in-lanes hop: groups of `lanes` RHS each block works through in turn
+  // 1: FP16 hop on the tensor cores (hop_mma_kernel) where its epilogue allows.  Selected only
+  // by WL_FORCE_TUNE: at 24^3x48 with 16 RHS it took 0.55-0.60 ms per hop against 0.28-0.29 ms
+  // for the 16-lane kernel (same iteration counts), latency-bound with the SM clock unthrottled,
+  // while this GPU's mma.sync m16n8k16 rate (about 440 TFLOP/s) was not the limit.
+  int mma = 0;
 };
 
 static dim3 grid_for(const Geom& g, const Tune& t, int nrhs, int npar) {
+  if (t.mma) return dim3((g.Vh + kMmaSites - 1) / kMmaSites, (nrhs + kMmaRhs - 1) / kMmaRhs, npar);
   if (t.lanes > 0) {
     const int S = kLaneBlock / t.lanes, per = t.lanes * std::max(1, t.seq);
     return dim3((g.Vh + S - 1) / S, (nrhs + per - 1) / per, npar);
@@ -264,8 +271,19 @@ static void launch_finalize(const Reduce& r, int nrhs, dim3 grid, const int* mas
 template <bool DAG, class IDX, class LF, class SF, class EPI>
 static void launch_hop_impl(const Tune& t, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st);
 
+// The tensor-core hop runs for FP16 fields on the compact layout behind epilogues that
+// have a per-colour form; any other launch with Tune::mma set uses the lanes kernel.
+template <class IDX, class SF, class EPI>
+static Tune effective_tune(Tune t) {
+  if (t.mma && !(std::is_same<SF, SpinorField<P_HALF>>::value && std::is_same<IDX, IdxCompact>::value &&
+                 HasSlice<EPI>::value))
+    t.mma = 0;
+  return t;
+}
+
 template <bool DAG, class IDX, class LF, class SF, class EPI>
-static void launch_hop(const Tune& t, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st) {
+static void launch_hop(const Tune& t0, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st) {
+  const Tune t = effective_tune<IDX, SF, EPI>(t0);
   launch_hop_impl<DAG, IDX>(t, a, npar, st);
   if (EPI::kReduce) {
     const bool lanes = (UsesFastHop<SF>::value || std::is_same<SF, SpinorField<P_DOUBLE>>::value) &&
@@ -298,6 +316,12 @@ static void launch_hop_impl(const Tune& t, const HopArgs<LF, SF, EPI>& a, int np
     }
   }
   if constexpr (UsesFastHop<SF>::value && std::is_same<IDX, IdxCompact>::value) {
+    if constexpr (std::is_same<SF, SpinorField<P_HALF>>::value && HasSlice<EPI>::value) {
+      if (t.mma) {
+        hop_mma_kernel<DAG><<<grid, dim3(kMmaWarps * 32, 1, 1), 0, st>>>(a);
+        return;
+      }
+    }
     if constexpr (std::is_same<SF, SpinorField<P_HALF>>::value) {
       if (t.lanes > 0 && half_color_enabled()) {  // colour multiply in packed FP16 (HFMA2)
         dim3 lb(kLaneBlock, 1, 1);
@@ -1731,17 +1755,20 @@ static Tune pick_update_tune(wl_engine* E, cudaStream_t st) {
 }
 
 static Tune pick_tune(wl_engine* E, cudaStream_t st) {
-  // WL_FORCE_TUNE="nr,bx,by,lanes[,pair]" pins the hop shape (tests exercise every shape this way)
+  // WL_FORCE_TUNE="nr,bx,by,lanes[,pair[,mma]]" pins the hop shape (tests exercise every shape this way)
   if (const char* f = std::getenv("WL_FORCE_TUNE")) {
     Tune t;
-    const int nf = std::sscanf(f, "%d,%d,%d,%d,%d", &t.nr, &t.bx, &t.by, &t.lanes, &t.pair);
+    const int nf = std::sscanf(f, "%d,%d,%d,%d,%d,%d", &t.nr, &t.bx, &t.by, &t.lanes, &t.pair, &t.mma);
     if (nf == 4) t.pair = 0;
+    if (nf < 6) t.mma = 0;
+    t.mma = t.mma ? 1 : 0;
     if (nf >= 4) {
       const bool lanes_ok = t.lanes == 0 || t.lanes == 4 || t.lanes == 8 || t.lanes == 16;
       const bool nr_ok = t.nr == 1 || t.nr == 2 || t.nr == 4;
       const bool shape_ok = t.bx % 32 == 0 && t.bx >= 64 && t.bx * t.by <= 256 && t.by * t.nr <= kMaxRB;
       if (lanes_ok && nr_ok && (t.lanes > 0 || shape_ok)) {
         if (t.lanes > 0 && !E->lanes_mode) t = Tune{};  // FP64 iteration or < 4 slots: thread-per-site kernel
+        if (t.mma && (t.lanes == 0 || E->sprec != P_HALF)) t.mma = 0;  // FP16 lanes engines only
         if (t.lanes > 0) t.bx = kLaneBlock;
         if (t.pair && (E->sprec != P_DOUBLE || E->lanes_mode || t.lanes > 0)) t.pair = 0;  // FP64 sites only
         if (t.pair) t.nr = 1, t.by = 1;
@@ -1771,8 +1798,8 @@ static Tune pick_tune(wl_engine* E, cudaStream_t st) {
   }
   const char* verb = std::getenv("WL_VERBOSE");
   if (verb && verb[0] == '1')
-    std::fprintf(stderr, "[wl] tune vh=%d prec=%d nslots=%d op=%d -> nr=%d bx=%d by=%d lanes=%d pair=%d\n", k.vh,
-                 k.prec, k.nslots, k.op, t.nr, t.bx, t.by, t.lanes, t.pair);
+    std::fprintf(stderr, "[wl] tune vh=%d prec=%d nslots=%d op=%d -> nr=%d bx=%d by=%d lanes=%d pair=%d mma=%d\n",
+                 k.vh, k.prec, k.nslots, k.op, t.nr, t.bx, t.by, t.lanes, t.pair, t.mma);
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune_cache[k] = t;
   return t;

@@ -8,7 +8,7 @@
 //   * spinors are structure-of-arrays per right-hand side:
 //       FP64: double2 [rhs][12][Vh]    (component k = spin*3 + colour)
 //       FP32: float4  [rhs][6][Vh]     (two complex components per float4)
-//       FP16: uint4   [rhs][3][Vh]     (eight halves = four complex) + float norm[rhs][Vh]
+//       FP16: uint4   [rhs][3][Vh]     (chunk = one colour, its four spins as half2) + float norm[rhs][Vh]
 //     so one warp's load of one chunk is 512 contiguous bytes.
 //   * links, split by the parity p of the site they start from:
 //       FP64/18: double2 [p][mu][9][Vh]   FP64/12: double2 [p][mu][6][Vh]
@@ -262,6 +262,10 @@ template <> struct SpinorField<P_SINGLE> : Strides {
   }
 };
 
+// FP16 record of one (site, rhs): three 16-byte chunks, chunk k = colour k with
+// the four spins as half2 (re, im), plus one float norm (value = norm * half).
+// The colour-major order lets the tensor-core hop give each lane of an MMA
+// group one colour of all four spins with a single 16-byte load.
 template <> struct SpinorField<P_HALF> : Strides {
   using real = float;
   uint4* ptr;
@@ -270,14 +274,13 @@ template <> struct SpinorField<P_HALF> : Strides {
   WL_D void load_impl(Spinor<float>& s, int rhs, long long c) const {
     float nrm = NC ? ldg(norm + nat(rhs, c)) : norm[nat(rhs, c)];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 3; ++k) {  // chunk k = colour k, spins 0..3
       uint4 v = NC ? ldg(ptr + at(rhs, k, c)) : ptr[at(rhs, k, c)];
       float2 a0 = h2f(v.x), a1 = h2f(v.y), a2 = h2f(v.z), a3 = h2f(v.w);
-      int i = 4 * k;
-      s.v[(i + 0) / 3][(i + 0) % 3] = {a0.x * nrm, a0.y * nrm};
-      s.v[(i + 1) / 3][(i + 1) % 3] = {a1.x * nrm, a1.y * nrm};
-      s.v[(i + 2) / 3][(i + 2) % 3] = {a2.x * nrm, a2.y * nrm};
-      s.v[(i + 3) / 3][(i + 3) % 3] = {a3.x * nrm, a3.y * nrm};
+      s.v[0][k] = {a0.x * nrm, a0.y * nrm};
+      s.v[1][k] = {a1.x * nrm, a1.y * nrm};
+      s.v[2][k] = {a2.x * nrm, a2.y * nrm};
+      s.v[3][k] = {a3.x * nrm, a3.y * nrm};
     }
   }
   WL_D void load(Spinor<float>& s, int rhs, long long c) const { load_impl<true>(s, rhs, c); }
@@ -297,11 +300,10 @@ template <> struct SpinorField<P_HALF> : Strides {
     norm[nat(rhs, c)] = keep ? mx : 0.f;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      int i = 4 * k;
-      const cplx<float>& c0 = s.v[(i + 0) / 3][(i + 0) % 3];
-      const cplx<float>& c1 = s.v[(i + 1) / 3][(i + 1) % 3];
-      const cplx<float>& c2 = s.v[(i + 2) / 3][(i + 2) % 3];
-      const cplx<float>& c3 = s.v[(i + 3) / 3][(i + 3) % 3];
+      const cplx<float>& c0 = s.v[0][k];
+      const cplx<float>& c1 = s.v[1][k];
+      const cplx<float>& c2 = s.v[2][k];
+      const cplx<float>& c3 = s.v[3][k];
       uint4 v;
       v.x = f2h(c0.re * inv, c0.im * inv);
       v.y = f2h(c1.re * inv, c1.im * inv);
@@ -344,12 +346,12 @@ template <> struct Packed<SpinorField<P_HALF>> {
   WL_D static float load(const SpinorField<P_HALF>& f, int rhs, unsigned c, float2 (&v)[12]) {
     const float n = ldg(f.norm + f.nat(rhs, c));
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 3; ++k) {  // chunk k = colour k, spins 0..3
       const uint4 q = ldg(f.ptr + f.at(rhs, k, c));
-      v[4 * k + 0] = h2f(q.x);
-      v[4 * k + 1] = h2f(q.y);
-      v[4 * k + 2] = h2f(q.z);
-      v[4 * k + 3] = h2f(q.w);
+      v[k] = h2f(q.x);
+      v[3 + k] = h2f(q.y);
+      v[6 + k] = h2f(q.z);
+      v[9 + k] = h2f(q.w);
     }
     return n;
   }
@@ -364,8 +366,8 @@ template <> struct Packed<SpinorField<P_HALF>> {
     const float2 s = f2(inv, inv);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const float2 a0 = fmul2(s, v[4 * k]), a1 = fmul2(s, v[4 * k + 1]);
-      const float2 a2 = fmul2(s, v[4 * k + 2]), a3 = fmul2(s, v[4 * k + 3]);
+      const float2 a0 = fmul2(s, v[k]), a1 = fmul2(s, v[3 + k]);
+      const float2 a2 = fmul2(s, v[6 + k]), a3 = fmul2(s, v[9 + k]);
       uint4 q;
       q.x = f2h(a0.x, a0.y);
       q.y = f2h(a1.x, a1.y);
@@ -383,6 +385,63 @@ WL_D double pnorm2(const float2 (&v)[12]) {
   for (int k = 0; k < 12; ++k) s = ffma2(v[k], v[k], s);
   return (double)s.x + (double)s.y;
 }
+
+WL_D double pnorm2_4(const float2 (&v)[4]) {
+  float2 s = f2(0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s = ffma2(v[k], v[k], s);
+  return (double)s.x + (double)s.y;
+}
+
+// One colour of an FP16 record (its four spins), for the tensor-core hop, whose
+// lanes hold one colour each: lanes t = 0, 1, 2 of an aligned group of four
+// share a record (colour t), lane t = 3 holds none (its values are zero).
+struct SliceHalf {
+  struct Raw {
+    uint4 q;
+    float n;
+  };
+  // the stored chunk and norm (zeros unless `mine`), issued early by the tensor-core hop
+  WL_D static Raw load(const SpinorField<P_HALF>& f, int rhs, unsigned c, int t, bool mine) {
+    Raw r{make_uint4(0u, 0u, 0u, 0u), 0.f};
+    if (mine) {
+      r.q = ldg(f.ptr + f.at(rhs, t, c));
+      r.n = ldg(f.norm + f.nat(rhs, c));
+    }
+    return r;
+  }
+  // v = stored values of colour t; returns the record's norm
+  WL_D static float unpack(const Raw& r, float2 (&v)[4]) {
+    v[0] = h2f(r.q.x);
+    v[1] = h2f(r.q.y);
+    v[2] = h2f(r.q.z);
+    v[3] = h2f(r.q.w);
+    return r.n;
+  }
+  // Every lane of the warp calls this (the norm is the max over the group's four
+  // lanes); `act` is uniform over a group, and only active groups write.
+  WL_D static void store(const SpinorField<P_HALF>& f, int rhs, unsigned c, int t, bool act, const float2 (&v)[4]) {
+    float mx = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mx = fmaxf(mx, fmaxf(fabsf(v[k].x), fabsf(v[k].y)));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+    // below FLT_MIN the record is stored as zero (1/mx would overflow, 0 * Inf = NaN)
+    const bool keep = mx >= 1.17549435e-38f;
+    const float inv = keep ? 1.0f / mx : 0.f;
+    if (act && t < 3) {
+      const float2 s = f2(inv, inv);
+      const float2 a0 = fmul2(s, v[0]), a1 = fmul2(s, v[1]), a2 = fmul2(s, v[2]), a3 = fmul2(s, v[3]);
+      uint4 q;
+      q.x = f2h(a0.x, a0.y);
+      q.y = f2h(a1.x, a1.y);
+      q.z = f2h(a2.x, a2.y);
+      q.w = f2h(a3.x, a3.y);
+      f.ptr[f.at(rhs, t, c)] = q;
+    }
+    if (act && t == 0) f.norm[f.nat(rhs, c)] = keep ? mx : 0.f;
+  }
+};
 
 // Spinor field in the reference layout: complex128 [rhs][V][4][3], site = flat index.
 struct SpinorRef {

@@ -491,6 +491,31 @@ struct EpiXpay {
     Packed<SF>::store(out[parity], rhs, idx, acc);
     return RED ? pnorm2(acc) : 0.0;
   }
+  // same on one colour of an FP16 record (tensor-core hop): slice_in issues the loads
+  // early, slice_out (called by every lane of the warp) finishes the record
+  struct SliceIn {
+    SliceHalf::Raw x;
+  };
+  WL_D SliceIn slice_in(int rhs, int parity, unsigned idx, int t, bool mine) const {
+    return SliceIn{SliceHalf::load(self[parity], rhs, idx, t, mine && has_self)};
+  }
+  WL_D double slice_out(const SliceIn& in, int rhs, int parity, unsigned idx, int t, bool act,
+                        float2 (&acc)[4]) const {
+    const float bb = act ? float(b ? b[rhs] : b0) : 0.f;
+    const float2 b2 = f2(bb, bb);
+    if (has_self) {
+      float2 x[4];
+      const float sx = SliceHalf::unpack(in.x, x) * (act ? float(a ? a[rhs] : a0) : 0.f);
+      const float2 s2 = f2(sx, sx);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[k] = ffma2(b2, acc[k], fmul2(s2, x[k]));
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[k] = fmul2(b2, acc[k]);
+    }
+    SliceHalf::store(out[parity], rhs, idx, t, act, acc);
+    return RED ? pnorm2_4(acc) : 0.0;
+  }
 };
 
 }  // namespace wl

@@ -30,12 +30,12 @@ template <> struct RawLoad<SpinorField<P_HALF>> {
   WL_D static float load(const SpinorField<P_HALF>& f, int rhs, long long c, float2 (&s)[12]) {
     const float n = ldg(f.norm + f.nat(rhs, c));
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 3; ++k) {  // chunk k = colour k, spins 0..3
       uint4 v = ldg(f.ptr + f.at(rhs, k, c));
-      s[4 * k + 0] = h2f(v.x);
-      s[4 * k + 1] = h2f(v.y);
-      s[4 * k + 2] = h2f(v.z);
-      s[4 * k + 3] = h2f(v.w);
+      s[k] = h2f(v.x);
+      s[3 + k] = h2f(v.y);
+      s[6 + k] = h2f(v.z);
+      s[9 + k] = h2f(v.w);
     }
     return n;
   }
@@ -326,7 +326,7 @@ WL_D void color_mul_smem(const LinkSmem& L, const float2 (&h)[6], float2 (&uh)[6
 // FP16 projection: the rank-2 projection is formed on the stored half2 values
 // (packed FP16 add/FMA, one rounding to FP16) and only the six projected
 // components are converted to FP32, instead of all twelve.  For mu = 3 the
-// projection is a selection and the unused third of the spinor is not loaded.
+// projection is a selection and the two unused spins are not loaded.
 // Measured at 24^3x48, 16 RHS: hop 0.329 -> 0.320 ms at a lower clock, CG
 // iteration and reliable-update counts unchanged (156-165, 16).
 #ifndef WL_HALF_PROJECT
@@ -335,20 +335,33 @@ WL_D void color_mul_smem(const LinkSmem& L, const float2 (&h)[6], float2 (&uh)[6
 
 WL_D __half2 as_h2(unsigned int u) { return *reinterpret_cast<__half2*>(&u); }
 
+// s[spin*3 + colour] of an FP16 record; for mu = 3 the projector keeps two spins
+// (0, 1 for C > 0, else 2, 3), so only those 8 bytes of each colour chunk are loaded.
+template <int MU, int C>
+WL_D void load_half_spins(const SpinorField<P_HALF>& f, int rhs, unsigned c, __half2 (&s)[12]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (MU == 3) {
+      const uint2* q = reinterpret_cast<const uint2*>(f.ptr + f.at(rhs, k, c)) + (C > 0 ? 0 : 1);
+      const uint2 v = __ldg(q);
+      s[(C > 0 ? 0 : 6) + k] = as_h2(v.x);
+      s[(C > 0 ? 3 : 9) + k] = as_h2(v.y);
+    } else {
+      const uint4 v = ldg(f.ptr + f.at(rhs, k, c));
+      s[k] = as_h2(v.x);
+      s[3 + k] = as_h2(v.y);
+      s[6 + k] = as_h2(v.z);
+      s[9 + k] = as_h2(v.w);
+    }
+  }
+}
+
 // the projection as half2 values (rows 0, 1 x colours), no conversion; returns the site norm
 template <int MU, int C>
 WL_D float load_project_half2(const SpinorField<P_HALF>& f, int rhs, unsigned c, __half2 (&h)[6]) {
   const float n = ldg(f.norm + f.nat(rhs, c));
   __half2 s[12];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    if (MU == 3 && ((C > 0 && k == 2) || (C < 0 && k == 0))) continue;
-    const uint4 v = ldg(f.ptr + f.at(rhs, k, c));
-    s[4 * k + 0] = as_h2(v.x);
-    s[4 * k + 1] = as_h2(v.y);
-    s[4 * k + 2] = as_h2(v.z);
-    s[4 * k + 3] = as_h2(v.w);
-  }
+  load_half_spins<MU, C>(f, rhs, c, s);
   const __half2 pcm = __floats2half2_rn((float)C, -(float)C);  // -iC x = pcm * swap(x)
   const __half2 pmc = __floats2half2_rn(-(float)C, (float)C);  //  iC x = pmc * swap(x)
 #pragma unroll
@@ -375,15 +388,7 @@ template <int MU, int C>
 WL_D float load_project_half(const SpinorField<P_HALF>& f, int rhs, unsigned c, float2 (&h)[6]) {
   const float n = ldg(f.norm + f.nat(rhs, c));
   __half2 s[12];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    if (MU == 3 && ((C > 0 && k == 2) || (C < 0 && k == 0))) continue;
-    const uint4 v = ldg(f.ptr + f.at(rhs, k, c));
-    s[4 * k + 0] = as_h2(v.x);
-    s[4 * k + 1] = as_h2(v.y);
-    s[4 * k + 2] = as_h2(v.z);
-    s[4 * k + 3] = as_h2(v.w);
-  }
+  load_half_spins<MU, C>(f, rhs, c, s);
   const __half2 pcm = __floats2half2_rn((float)C, -(float)C);  // -iC x = pcm * swap(x)
   const __half2 pmc = __floats2half2_rn(-(float)C, (float)C);  //  iC x = pmc * swap(x)
 #pragma unroll
@@ -496,6 +501,43 @@ WL_D void lane_dir_hc(const SpinorField<P_HALF>& src, const LinkSmem* Ls, const 
   }
 }
 
+// Link q = 2 mu + dir of target site c (compact index, target parity) with the
+// boundary phase folded in, staged as FP32 quads (re, re, -im, im) or, for the
+// FP16 colour multiply (HC), as two half2 (re, re), (-+im, +-im) (backward hops
+// stage the conjugate); returns the compact index of the neighbour it hops to.
+template <bool HC, class LF, class DST>
+WL_D int stage_link(const Geom& g, const LF& links, int parity, int c, int mu, int dir, DST& dst) {
+  const Site s = site_from_compact(g, parity, c);
+  const int nb = neighbor(g, s, mu, dir == 0 ? +1 : -1);
+  Link<float> u;
+  if (dir == 0) links.load(u, parity, mu, c);
+  else links.load(u, 1 - parity, mu, nb);
+  // the forward hop from x_mu = L-1 uses ph*U; the backward hop into
+  // x_mu = 0 uses (ph*U)^dag, i.e. the same phase-multiplied link
+  const bool ph = g.ph_on[mu] && (dir == 0 ? (s.x[mu] == g.L[mu] - 1) : (s.x[mu] == 0));
+  if (ph) {
+    const cplx<float> w{(float)g.ph_re[mu], (float)g.ph_im[mu]};
+#pragma unroll
+    for (int k = 0; k < 9; ++k) u.m[k / 3][k % 3] = u.m[k / 3][k % 3] * w;
+  }
+  if constexpr (HC) {
+    LinkSmemH* lh = reinterpret_cast<LinkSmemH*>(&dst);
+    const float sgn = dir == 0 ? 1.0f : -1.0f;  // backward hops use the conjugate
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const cplx<float> v = u.m[k / 3][k % 3];
+      lh->p[k] = make_uint2(f2h(v.re, v.re), f2h(-sgn * v.im, sgn * v.im));
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const cplx<float> v = u.m[k / 3][k % 3];
+      dst.p[k] = make_float4(v.re, v.re, -v.im, v.im);
+    }
+  }
+  return nb;
+}
+
 // Per-block partial sums: xor-shuffles over the sites of a warp leave lanes
 // 0..R-1 with the warp's sum for RHS rbase + lane; after one barrier threads
 // 0..R-1 add the block's warps in a fixed order and block b writes
@@ -541,35 +583,7 @@ __global__ void __launch_bounds__(kLaneBlock, LaneMinBlocks<DAG, EPI>::value) ho
     const int sl = wsite + (j >> 3), q = j & 7, mu = q >> 1, dir = q & 1;
     const int c = site0 + sl;
     if (c < A.g.Vh) {
-      const Site s = site_from_compact(A.g, parity, c);
-      const int nb = neighbor(A.g, s, mu, dir == 0 ? +1 : -1);
-      Link<float> u;
-      if (dir == 0) A.links.load(u, parity, mu, c);
-      else A.links.load(u, 1 - parity, mu, nb);
-      // the forward hop from x_mu = L-1 uses ph*U; the backward hop into
-      // x_mu = 0 uses (ph*U)^dag, i.e. the same phase-multiplied link
-      const bool ph = A.g.ph_on[mu] && (dir == 0 ? (s.x[mu] == A.g.L[mu] - 1) : (s.x[mu] == 0));
-      if (ph) {
-        const cplx<float> w{(float)A.g.ph_re[mu], (float)A.g.ph_im[mu]};
-#pragma unroll
-        for (int k = 0; k < 9; ++k) u.m[k / 3][k % 3] = u.m[k / 3][k % 3] * w;
-      }
-      if constexpr (HC) {
-        LinkSmemH* lh = reinterpret_cast<LinkSmemH*>(&sm.link[sl].l[q]);
-        const float sgn = dir == 0 ? 1.0f : -1.0f;  // backward hops use the conjugate
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          const cplx<float> v = u.m[k / 3][k % 3];
-          lh->p[k] = make_uint2(f2h(v.re, v.re), f2h(-sgn * v.im, sgn * v.im));
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          const cplx<float> v = u.m[k / 3][k % 3];
-          sm.link[sl].l[q].p[k] = make_float4(v.re, v.re, -v.im, v.im);
-        }
-      }
-      sm.nb[sl][q] = nb;
+      sm.nb[sl][q] = stage_link<HC>(A.g, A.links, parity, c, mu, dir, sm.link[sl].l[q]);
       if (q == 0) sm.ok[sl] = 1;
     } else if (q == 0) {
       sm.ok[sl] = 0;

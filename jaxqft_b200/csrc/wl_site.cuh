@@ -253,6 +253,46 @@ struct EpiCG {
     }
     return n;
   }
+  // same on one colour of an FP16 record (tensor-core hop): slice_in issues the four
+  // loads early, slice_out (called by every lane of the warp) finishes the records
+  struct SliceIn {
+    SliceHalf::Raw y, r, p, x;
+  };
+  WL_D SliceIn slice_in(int rhs, int parity, unsigned idx, int t, bool mine) const {
+    return SliceIn{SliceHalf::load(y[parity], rhs, idx, t, mine), SliceHalf::load(rs[parity], rhs, idx, t, mine),
+                   SliceHalf::load(p[parity], rhs, idx, t, mine), SliceHalf::load(xs[parity], rhs, idx, t, mine)};
+  }
+  WL_D double slice_out(const SliceIn& in, int rhs, int parity, unsigned idx, int t, bool act,
+                        float2 (&acc)[4]) const {
+    const float al = act ? float(alpha[rhs]) : 0.f;
+    const float bb = act ? float(b[rhs]) : 0.f, aa = act ? float(a[rhs]) : 0.f;
+    const float2 b2 = f2(bb, bb), nal = f2(-al, -al);
+    float2 v[4];
+    {  // acc <- Ap = a*y + b*acc
+      const float sy = SliceHalf::unpack(in.y, v) * aa;
+      const float2 s2 = f2(sy, sy);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[k] = ffma2(b2, acc[k], fmul2(s2, v[k]));
+    }
+    double n;
+    {  // rs <- rs - alpha Ap
+      const float sr = SliceHalf::unpack(in.r, v);
+      const float2 s2 = f2(sr, sr);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] = ffma2(nal, acc[k], fmul2(s2, v[k]));
+      SliceHalf::store(rs[parity], rhs, idx, t, act, v);
+      n = pnorm2_4(v);
+    }
+    {  // xs <- xs + alpha p
+      const float sp = SliceHalf::unpack(in.p, acc) * al;
+      const float sx = SliceHalf::unpack(in.x, v);
+      const float2 p2 = f2(sp, sp), x2 = f2(sx, sx);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] = ffma2(p2, acc[k], fmul2(x2, v[k]));
+      SliceHalf::store(xs[parity], rhs, idx, t, act, v);
+    }
+    return n;
+  }
 };
 
 // Last hop of the FP64 normal operator on x64, giving the true residual:

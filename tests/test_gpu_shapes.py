@@ -1,6 +1,7 @@
 """Every hop kernel shape the autotuner can choose, pinned with WL_FORCE_TUNE:
-classic thread-per-site kernels with 1/2/4 RHS per thread and the RHS-in-lanes
-kernel with 4/8/16 lanes per site.  Each shape must give the same operator
+classic thread-per-site kernels with 1/2/4 RHS per thread, the RHS-in-lanes
+kernel with 4/8/16 lanes per site and the tensor-core FP16 hop (last shape; FP32
+engines run the 16-lane kernel for it).  Each shape must give the same operator
 (FP32: 2e-6, FP16: 4e-3 of FP64) and batched solves that reach an FP64 true
 residual <= 1e-10 and agree with standalone FP64 solves."""
 
@@ -19,7 +20,7 @@ if not torch.cuda.is_available():  # pragma: no cover
 
 from jaxqft_b200.lib import Engine, WilsonContext  # noqa: E402
 
-SHAPES = ["1,128,1,0", "2,64,2,0", "4,64,4,0", "1,128,1,4", "1,128,1,8", "1,128,1,16"]
+SHAPES = ["1,128,1,0", "2,64,2,0", "4,64,4,0", "1,128,1,4", "1,128,1,8", "1,128,1,16", "1,128,1,16,0,1"]
 TOLS = {"single": 2e-6, "half": 4e-3}
 
 
