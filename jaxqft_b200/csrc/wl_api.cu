@@ -219,10 +219,12 @@ struct Tune {
   int lanes = 0;  // > 0: RHS-in-lanes hop (FP16/FP32 storage) with this many RHS lanes per site
   int pair = 0;   // 1: FP64 single-RHS stencil with two threads per site (hop_pair_kernel)
   int seq = 1;    // FP64 RHS-in-lanes hop: groups of `lanes` RHS each block works through in turn
-  // 1: FP16 hop on the tensor cores (hop_mma_kernel) where its epilogue allows.  Selected only
-  // by WL_FORCE_TUNE: at 24^3x48 with 16 RHS it took 0.55-0.60 ms per hop against 0.28-0.29 ms
-  // for the 16-lane kernel (same iteration counts), latency-bound with the SM clock unthrottled,
-  // while this GPU's mma.sync m16n8k16 rate (about 440 TFLOP/s) was not the limit.
+  // 1: FP16 hop on the tensor cores (hop_mma_kernel, 16 RHS per warp) where its epilogue
+  // allows.  Selected only by WL_FORCE_TUNE: at 24^3x48 with 16 RHS it takes 0.45 ms per hop
+  // against 0.28 ms for the 16-lane kernel (same iteration counts).  It moves the colour
+  // multiply to the tensor pipe (7 % busy) but executes about 800 warp instructions per site
+  // (record fetch, relative weights, per-colour epilogue) against 650 for the lanes kernel, with
+  // 12 resident warps per SM instead of 28, so it issues on 46 % of cycles.
   int mma = 0;
 };
 
@@ -249,6 +251,16 @@ static bool half_color_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("WL_HALF_COLOR");
     return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// WL_HALF_ACC=1: the 16-lane FP16 hop also accumulates its eight contributions in packed FP16
+// (relative weights, lane_site_hh), for comparisons.
+static bool half_acc_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("WL_HALF_ACC");
+    return e && e[0] == '1';
   }();
   return on;
 }
@@ -318,13 +330,22 @@ static void launch_hop_impl(const Tune& t, const HopArgs<LF, SF, EPI>& a, int np
   if constexpr (UsesFastHop<SF>::value && std::is_same<IDX, IdxCompact>::value) {
     if constexpr (std::is_same<SF, SpinorField<P_HALF>>::value && HasSlice<EPI>::value) {
       if (t.mma) {
-        hop_mma_kernel<DAG><<<grid, dim3(kMmaWarps * 32, 1, 1), 0, st>>>(a);
+        // 64 KB of dynamic shared memory per block (two record slots and the links of each
+        // warp); the opt-in is set once per instantiation
+        static const cudaError_t attr = cudaFuncSetAttribute(
+            hop_mma_kernel<DAG, LF, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMmaSmemBytes);
+        (void)attr;
+        hop_mma_kernel<DAG><<<grid, dim3(kMmaWarps * 32, 1, 1), kMmaSmemBytes, st>>>(a);
         return;
       }
     }
     if constexpr (std::is_same<SF, SpinorField<P_HALF>>::value) {
       if (t.lanes > 0 && half_color_enabled()) {  // colour multiply in packed FP16 (HFMA2)
         dim3 lb(kLaneBlock, 1, 1);
+        if (t.lanes == 16 && half_acc_enabled()) {
+          hop_lanes_kernel<DAG, 16, LF, SF, EPI, true, true><<<grid, lb, 0, st>>>(a);
+          return;
+        }
         switch (t.lanes) {
           case 16: hop_lanes_kernel<DAG, 16, LF, SF, EPI, true><<<grid, lb, 0, st>>>(a); break;
           case 8: hop_lanes_kernel<DAG, 8, LF, SF, EPI, true><<<grid, lb, 0, st>>>(a); break;

@@ -356,10 +356,20 @@ WL_D void load_half_spins(const SpinorField<P_HALF>& f, int rhs, unsigned c, __h
   }
 }
 
+// the projection as half2 values (rows 0, 1 x colours), no conversion and no norm
+template <int MU, int C>
+WL_D void load_project_half2_raw(const SpinorField<P_HALF>& f, int rhs, unsigned c, __half2 (&h)[6]);
+
 // the projection as half2 values (rows 0, 1 x colours), no conversion; returns the site norm
 template <int MU, int C>
 WL_D float load_project_half2(const SpinorField<P_HALF>& f, int rhs, unsigned c, __half2 (&h)[6]) {
   const float n = ldg(f.norm + f.nat(rhs, c));
+  load_project_half2_raw<MU, C>(f, rhs, c, h);
+  return n;
+}
+
+template <int MU, int C>
+WL_D void load_project_half2_raw(const SpinorField<P_HALF>& f, int rhs, unsigned c, __half2 (&h)[6]) {
   __half2 s[12];
   load_half_spins<MU, C>(f, rhs, c, s);
   const __half2 pcm = __floats2half2_rn((float)C, -(float)C);  // -iC x = pcm * swap(x)
@@ -381,7 +391,6 @@ WL_D float load_project_half2(const SpinorField<P_HALF>& f, int rhs, unsigned c,
       h[3 + col] = C > 0 ? s1 : s3;
     }
   }
-  return n;
 }
 
 template <int MU, int C>
@@ -455,8 +464,23 @@ struct LinkSmemH {
   uint2 p[9];  // (re, re), (-+im, +-im) as half2 pairs
 };
 
+// The nine link pairs of a hop, read from the start of its 16-byte aligned LinkSmem
+// slot as four 128-bit and one 64-bit shared loads instead of nine 64-bit ones.
+WL_D void load_link_pairs(const LinkSmem& slot, uint2 (&e)[9]) {
+  const uint4* L4 = reinterpret_cast<const uint4*>(&slot);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint4 v = L4[i];
+    e[2 * i] = make_uint2(v.x, v.y);
+    e[2 * i + 1] = make_uint2(v.z, v.w);
+  }
+  e[8] = reinterpret_cast<const LinkSmemH*>(&slot)->p[8];
+}
+
 template <bool DAGU>
-WL_D void color_mul_half(const LinkSmemH& L, const __half2 (&h)[6], float2 (&uh)[6]) {
+WL_D void color_mul_half(const LinkSmem& L, const __half2 (&h)[6], float2 (&uh)[6]) {
+  uint2 e[9];
+  load_link_pairs(L, e);
 #pragma unroll
   for (int sp = 0; sp < 2; ++sp) {
     __half2 hs[3];
@@ -467,7 +491,7 @@ WL_D void color_mul_half(const LinkSmemH& L, const __half2 (&h)[6], float2 (&uh)
       __half2 acc = __float2half2_rn(0.f);
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
-        const uint2 q = DAGU ? L.p[b * 3 + a] : L.p[a * 3 + b];
+        const uint2 q = DAGU ? e[b * 3 + a] : e[a * 3 + b];
         acc = __hfma2(as_h2(q.x), h[sp * 3 + b], acc);
         acc = __hfma2(as_h2(q.y), hs[b], acc);
       }
@@ -490,7 +514,7 @@ WL_D void lane_dir_hc(const SpinorField<P_HALF>& src, const LinkSmem* Ls, const 
     float2 uh[6];
     const float n = (dir == 0 ? load_project_half2<MU, CF>(src, rhs, (unsigned)nbs[q], h)
                               : load_project_half2<MU, CB>(src, rhs, (unsigned)nbs[q], h)) * W3;
-    const LinkSmemH& L = *reinterpret_cast<const LinkSmemH*>(&Ls[q]);
+    const LinkSmem& L = Ls[q];
     if (dir == 0) {
       color_mul_half<false>(L, h, uh);
       accum2<MU, CF>(acc, uh, n);
@@ -499,6 +523,118 @@ WL_D void lane_dir_hc(const SpinorField<P_HALF>& src, const LinkSmem* Ls, const 
       accum2<MU, CB>(acc, uh, n);
     }
   }
+}
+
+// FP16 accumulation.  The eight contributions of a site are summed in packed
+// FP16 with weights relative to the largest neighbour norm of this (site, RHS):
+// w_q = n_q / max n (times the factor 2 of mu = 3), so every weight is in
+// [0, 2] and the sums stay far inside the FP16 range (|U h| <= 2 sqrt 3 per
+// component); the FP32 result is the FP16 sum times max n.  This drops the six
+// half2 -> FP32 conversions per hop, and the accumulation is one HFMA2 per
+// complex term with the +-1 / +-i reconstruction folded into the weight pair.
+template <bool DAGU>
+WL_D void color_mul_hh(const LinkSmem& L, const __half2 (&h)[6], __half2 (&uh)[6]) {
+  uint2 e[9];
+  load_link_pairs(L, e);
+#pragma unroll
+  for (int sp = 0; sp < 2; ++sp) {
+    __half2 hs[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) hs[b] = __lowhigh2highlow(h[sp * 3 + b]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      __half2 acc = __float2half2_rn(0.f);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const uint2 q = DAGU ? e[b * 3 + a] : e[a * 3 + b];
+        acc = __hfma2(as_h2(q.x), h[sp * 3 + b], acc);
+        acc = __hfma2(as_h2(q.y), hs[b], acc);
+      }
+      uh[sp * 3 + a] = acc;
+    }
+  }
+}
+
+template <int MU, int C>
+WL_D void accum2_hh(__half2 (&acc)[12], const __half2 (&uh)[6], float w) {
+  const __half2 ww = __float2half2_rn(w);
+  const __half2 cw = __float2half2_rn(C * w);
+  const __half2 pcm = __floats2half2_rn(C * w, -C * w);  // -iC w x = pcm * swap(x)
+  const __half2 pmc = __floats2half2_rn(-C * w, C * w);  //  iC w x = pmc * swap(x)
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const __half2 u0 = uh[c], u1 = uh[3 + c];
+    if (MU == 3) {
+      if (C > 0) {
+        acc[c] = __hfma2(ww, u0, acc[c]);
+        acc[3 + c] = __hfma2(ww, u1, acc[3 + c]);
+      } else {
+        acc[6 + c] = __hfma2(ww, u0, acc[6 + c]);
+        acc[9 + c] = __hfma2(ww, u1, acc[9 + c]);
+      }
+      continue;
+    }
+    acc[c] = __hfma2(ww, u0, acc[c]);
+    acc[3 + c] = __hfma2(ww, u1, acc[3 + c]);
+    if (MU == 0) {
+      acc[6 + c] = __hfma2(cw, u1, acc[6 + c]);
+      acc[9 + c] = __hfma2(cw, u0, acc[9 + c]);
+    } else if (MU == 1) {
+      acc[6 + c] = __hfma2(pcm, __lowhigh2highlow(u1), acc[6 + c]);  // -iC u1
+      acc[9 + c] = __hfma2(pmc, __lowhigh2highlow(u0), acc[9 + c]);  //  iC u0
+    } else {
+      acc[6 + c] = __hfma2(pmc, __lowhigh2highlow(u0), acc[6 + c]);  //  iC u0
+      acc[9 + c] = __hfma2(pmc, __lowhigh2highlow(u1), acc[9 + c]);  //  iC u1
+    }
+  }
+}
+
+// w[q]: the relative weights of the site's eight neighbours for this RHS
+template <int MU, bool DAG>
+WL_D void lane_dir_hh(const SpinorField<P_HALF>& src, const LinkSmem* Ls, const int* nbs, int rhs,
+                      const float (&w)[8], __half2 (&acc)[12]) {
+  constexpr int CF = DAG ? +1 : -1;
+  constexpr int CB = -CF;
+#pragma unroll
+  for (int dir = 0; dir < 2; ++dir) {
+    const int q = 2 * MU + dir;
+    __half2 h[6], uh[6];
+    if (dir == 0) load_project_half2_raw<MU, CF>(src, rhs, (unsigned)nbs[q], h);
+    else load_project_half2_raw<MU, CB>(src, rhs, (unsigned)nbs[q], h);
+    const LinkSmem& L = Ls[q];
+    if (dir == 0) {
+      color_mul_hh<false>(L, h, uh);
+      accum2_hh<MU, CF>(acc, uh, w[q]);
+    } else {
+      color_mul_hh<true>(L, h, uh);
+      accum2_hh<MU, CB>(acc, uh, w[q]);
+    }
+  }
+}
+
+// The whole stencil of one (site, RHS) with FP16 accumulation; acc = FP32 result.
+template <bool DAG>
+WL_D void lane_site_hh(const SpinorField<P_HALF>& src, const LinkSmem* Ls, const int* nbs, int rhs,
+                       float2 (&acc)[12]) {
+  float w[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) w[q] = ldg(src.norm + src.nat(rhs, (unsigned)nbs[q]));
+  float m = 0.f;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) m = fmaxf(m, w[q]);
+  const float im = m > 0.f ? 1.0f / m : 0.f;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) w[q] *= (q >= 6 ? 2.0f * im : im);
+  __half2 ah[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) ah[k] = __float2half2_rn(0.f);
+  lane_dir_hh<0, DAG>(src, Ls, nbs, rhs, w, ah);
+  lane_dir_hh<1, DAG>(src, Ls, nbs, rhs, w, ah);
+  lane_dir_hh<2, DAG>(src, Ls, nbs, rhs, w, ah);
+  lane_dir_hh<3, DAG>(src, Ls, nbs, rhs, w, ah);
+  const float2 m2 = f2(m, m);
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = fmul2(m2, __half22float2(ah[k]));
 }
 
 // Link q = 2 mu + dir of target site c (compact index, target parity) with the
@@ -566,9 +702,10 @@ WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* /*mask*/
   }
 }
 
-template <bool DAG, int R, class LF, class SF, class EPI, bool HC = false>
+template <bool DAG, int R, class LF, class SF, class EPI, bool HC = false, bool HA = false>
 __global__ void __launch_bounds__(kLaneBlock, LaneMinBlocks<DAG, EPI>::value) hop_lanes_kernel(HopArgs<LF, SF, EPI> A) {
   static_assert(!HC || std::is_same<SF, SpinorField<P_HALF>>::value, "FP16 colour multiply needs FP16 fields");
+  static_assert(!HA || HC, "FP16 accumulation runs behind the FP16 colour multiply");
   constexpr int S = kLaneBlock / R;
   __shared__ LaneSmem<R> sm;
   const int tid = threadIdx.x;
@@ -602,7 +739,9 @@ __global__ void __launch_bounds__(kLaneBlock, LaneMinBlocks<DAG, EPI>::value) ho
     for (int k = 0; k < 12; ++k) acc[k] = f2(0.f, 0.f);
     const SF& src = A.src[1 - parity];
     const int* nbs = sm.nb[sl];
-    if constexpr (HC) {
+    if constexpr (HA) {
+      lane_site_hh<DAG>(src, sm.link[sl].l, nbs, rhs, acc);
+    } else if constexpr (HC) {
       const LinkSmem* Ls = sm.link[sl].l;
       lane_dir_hc<0, DAG>(src, Ls, nbs, rhs, acc);
       lane_dir_hc<1, DAG>(src, Ls, nbs, rhs, acc);

@@ -1,17 +1,21 @@
 """Host-side restatement of the tensor-core FP16 hop (jaxqft_b200/csrc/wl_hop_mma.cuh), no GPU.
 
-The kernel computes one site's hop over 8 RHS as 8 mma.sync m16n8k16 tiles
-(2 spin pairs x 4 mu; tile j holds RHS 0-7 of output spin 2j in rows 0-7 and
-of spin 2j + 1 in rows 8-15), each lane (g, t) holding colour t of RHS g.
-This test rebuilds, in float64, every lane's A words (``mma_rows``), B words
-(staged link pairs + ``__byte_perm`` selection) and the per-tile matrices of the
-PTX fragment layout of m16n8k16 (A: rows g / g + 8, columns 2t, 2t + 1 and
-2t + 8, 2t + 9; B: rows 2t, 2t + 1 and 2t + 8, 2t + 9, column g; D: rows g /
-g + 8, columns 2t, 2t + 1), multiplies them, and reads the lanes' D fragments
-back as (RHS, spin, colour).  The result must equal the hop written the way
-the FP32 lanes kernel computes it: the rank-2 projection (project2), the
-colour multiply by U (forward) or U^dag (backward), and the reconstruction
-(accum2), weighted by the FP16 record norms and the factor 2 of mu = 3.
+The kernel computes one site's hop over 16 RHS as 16 mma.sync m16n8k16 tiles:
+for each mu, four output-spin tiles whose rows are the 16 RHS and whose K holds
+the forward and backward hop's projected colour components; lane (g, t) holds
+colour t of RHS g and g + 8.  This test rebuilds, in float64, every lane's A
+words (``mma_project``: weighted rank-2 projection), B words (``bword`` of the
+staged link element, its dagger for the backward hop, and the lower spins'
+coefficient ``cmul_unit<LowerKappa>``), the per-tile matrices of the PTX
+fragment layout of m16n8k16 (A: rows g / g + 8, columns 2t, 2t + 1 and 2t + 8,
+2t + 9; B: rows 2t, 2t + 1 and 2t + 8, 2t + 9, column g; D: rows g / g + 8,
+columns 2t, 2t + 1), multiplies them, and reads the lanes' D fragments back as
+(RHS, spin, colour).  The result must equal the hop written the way the FP32
+lanes kernel computes it: the rank-2 projection (project2), the colour
+multiply by U (forward) or U^dag (backward), and the reconstruction (accum2),
+weighted by the FP16 record norms and the factor 2 of mu = 3.  The shared
+memory layout (record slots with the r ^ 2t swizzle) and the cp.async
+assignment are checked too.
 """
 
 import numpy as np
@@ -52,50 +56,61 @@ def accum2(mu, C, acc, uh, w):
         acc[3] += 1j * C * w * u1
 
 
-def mma_rows(mu, C, v, w):
-    """the kernel's A words for output spins 0..3 (complex numbers); v = spins 0..3 of one colour."""
-    s0, s1, s2, s3 = v
+def proj_rows(mu, C, v, w):
+    """the kernel's A words of one record chunk: w * rows 0, 1 of (1 + C g_mu) psi (``mma_project``)."""
+    h0, h1 = project2(mu, C, v)
+    return w * h0, w * h1
+
+
+KAPPA = {0: 1, 1: -1, 2: 1j, 3: -1j}  # cmul_unit<K>
+
+
+def lower_kappa(mu, C):
+    """``LowerKappa``: coefficient of the lower spins, mu = 0: C, mu = 1: -iC, mu = 2: iC."""
     if mu == 0:
-        h0, h1 = s0 + C * s3, s1 + C * s2
-    elif mu == 1:
-        h0, h1 = s0 - 1j * C * s3, s1 + 1j * C * s2
-    elif mu == 2:
-        h0, h1 = s0 - 1j * C * s2, s1 - 1j * C * s3
-    else:
-        h0, h1 = (s0, s1) if C > 0 else (s2, s3)
-    h0, h1 = w * h0, w * h1
-    if mu == 3:
-        return [h0, h1, 0, 0] if C > 0 else [0, 0, h0, h1]
-    if mu == 0:
-        return [h0, h1, C * h1, C * h0]
+        return 0 if C > 0 else 1
     if mu == 1:
-        return [h0, h1, -1j * C * h1, 1j * C * h0]
-    return [h0, h1, 1j * C * h0, 1j * C * h1]
+        return 3 if C > 0 else 2
+    return 2 if C > 0 else 3
 
 
-def byte_perm_halves(x, y, sel):
-    """__byte_perm on words given as (lo, hi) half pairs: 0x5410 -> (x.lo, y.lo), 0x3276 -> (y.hi, x.hi)."""
-    if sel == 0x5410:
-        return (x[0], y[0])
-    assert sel == 0x3276
-    return (y[1], x[1])
+def bword(e, imc):
+    """B word of a lane for complex element e: column (a, re) -> (re, -im), column (a, im) -> (im, re)."""
+    return (e.imag, e.real) if imc else (e.real, -e.imag)
+
+
+def swizzle_ok():
+    """chunk (q, t, r) stored at RHS index r ^ 2t: a permutation, and the 16-byte reads of each
+    quarter-warp (8 lanes: g in {2p, 2p+1}, t in 0..2) hit distinct 16-byte bank groups."""
+    for t in range(3):
+        assert sorted(r ^ (2 * t) for r in range(16)) == list(range(16))
+    for p in range(4):
+        for hi in (0, 8):
+            groups = [((g + hi) ^ (2 * t)) % 8 for g in (2 * p, 2 * p + 1) for t in range(3)]
+            assert len(set(groups)) == len(groups)
+
+
+def test_smem_swizzle_conflict_free():
+    swizzle_ok()
 
 
 @pytest.mark.parametrize("dag", [False, True])
-@pytest.mark.parametrize("nact", [8, 5])
+@pytest.mark.parametrize("nact", [16, 11])
 def test_lane_fragments_reproduce_the_hop(dag, nact):
     rng = np.random.default_rng(7 + dag + nact)
     CF = 1 if dag else -1
-    psi = rng.normal(size=(8, 8, 4, 3)) + 1j * rng.normal(size=(8, 8, 4, 3))  # [hop][rhs][spin][colour]
-    norm = rng.uniform(0.1, 3.0, size=(8, 8))
+    NR = 16
+    psi = rng.normal(size=(8, NR, 4, 3)) + 1j * rng.normal(size=(8, NR, 4, 3))  # [hop][rhs][spin][colour]
+    norm = rng.uniform(0.1, 3.0, size=(8, NR))
     norm[:, 3] *= 1e-3  # a RHS whose neighbours differ widely in scale
     norm[2, 4] *= 1e-5
-    U = rng.normal(size=(8, 3, 3)) + 1j * rng.normal(size=(8, 3, 3))  # link of hop q (backward: U(x - mu))
-    act = np.arange(8) < nact
+    norm[5, 12] *= 1e-4
+    U = rng.normal(size=(8, 3, 3)) + 1j * rng.normal(size=(8, 3, 3))  # staged link of hop q (backward: U(x - mu))
+    act = np.arange(NR) < nact
 
     # reference: the lanes kernel's formulas
-    ref = np.zeros((8, 4, 3), dtype=complex)
-    for r in range(8):
+    ref = np.zeros((NR, 4, 3), dtype=complex)
+    for r in range(NR):
         if not act[r]:
             continue
         for q in range(8):
@@ -106,70 +121,88 @@ def test_lane_fragments_reproduce_the_hop(dag, nact):
             uh = np.array([Uop @ h[0], Uop @ h[1]])
             accum2(mu, C, ref[r], uh, norm[q, r] * (2.0 if mu == 3 else 1.0))
 
-    # staged link pairs: element k = (a, b) -> x = (re, re), y = (-sgn im, sgn im), sgn = -1 backward
-    def staged(q, k):
-        v = U[q][k // 3, k % 3]
-        sgn = -1.0 if q % 2 else 1.0
-        return (v.real, v.real), (-sgn * v.imag, sgn * v.imag)
-
-    m = np.where(act, norm.max(axis=0), 0.0)  # per-RHS scale (max over the 8 hops)
-    D = np.zeros((2, 32, 4))  # [tile][lane][c0..c3]
+    nrm = np.where(act[None, :], norm, 0.0)  # zero-filled norms of inactive RHS
+    m = nrm.max(axis=0)
+    inv = np.where(m > 0, 1.0 / np.where(m > 0, m, 1.0), 0.0)
+    D = np.zeros((4, 32, 4))  # [spin tile][lane][d0..d3]
     for mu in range(4):
-        Afull = np.zeros((2, 16, 16))
-        Bfull = np.zeros((16, 8))
+        qf, qb = 2 * mu, 2 * mu + 1
+        A = np.zeros((2, 16, 16))  # row tiles 0, 1
+        B = {k: np.zeros((16, 8)) for k in ("up", "lo", "lo_neg")}
         for lane in range(32):
             g, t = lane >> 2, lane & 3
-            r = g
-            ca = g >> 1
-            bval = ca < 3 and t < 3
-            sel = 0x3276 if g & 1 else 0x5410
-            kf, kb = (ca * 3 + t, t * 3 + ca) if bval else (0, 0)
-            words = {}
-            for back in (0, 1):
-                q = 2 * mu + back
-                C = -CF if back else CF
-                on = act[r] and t < 3
-                v = psi[q, r, :, t] if on else np.zeros(4)
-                w = norm[q, r] / m[r] * (2.0 if mu == 3 else 1.0) if act[r] else 0.0
-                words[back] = mma_rows(mu, C, v, w)
-            bw = []
-            for back, k in ((0, kf), (1, kb)):
-                x, y = staged(2 * mu + back, k)
-                bw.append(byte_perm_halves(x, y, sel) if bval else (0.0, 0.0))
-            # a0 = (row g, cols 2t..), a1 = (row g + 8, cols 2t..), a2 = (row g, cols 2t + 8..), a3 = (row g + 8, ..)
-            for j in range(2):
-                for row, col, z in ((g, 2 * t, words[0][2 * j]), (g + 8, 2 * t, words[0][2 * j + 1]),
-                                    (g, 2 * t + 8, words[1][2 * j]), (g + 8, 2 * t + 8, words[1][2 * j + 1])):
-                    z = complex(z)
-                    Afull[j, row, col] = z.real
-                    Afull[j, row, col + 1] = z.imag
-            for back in (0, 1):
-                lo, hi = bw[back]
-                Bfull[2 * t + 8 * back, g] = lo
-                Bfull[2 * t + 8 * back + 1, g] = hi
-        for j in range(2):
-            Dt = Afull[j] @ Bfull
+            # A words (rows g, g + 8; forward cols 2t.., backward cols 2t + 8..)
+            if t < 3:
+                for row, r in ((g, g), (g + 8, g + 8)):
+                    for q, col0 in ((qf, 0), (qb, 8)):
+                        C = CF if q == qf else -CF
+                        v = psi[q, r, :, t] if act[r] else np.zeros(4)
+                        w = nrm[q, r] * inv[r] * (2.0 if mu == 3 else 1.0)
+                        h0, h1 = proj_rows(mu, C, v, w)
+                        for j, h in ((0, h0), (1, h1)):
+                            A[j, row, col0 + 2 * t] = h.real
+                            A[j, row, col0 + 2 * t + 1] = h.imag
+            # B words: column g, rows 2t, 2t + 1 (forward) and 2t + 8, 2t + 9 (backward)
+            a, imc = g >> 1, g & 1
+            uf = U[qf][a, t] if (a < 3 and t < 3) else 0.0
+            vb = np.conj(U[qb][t, a]) if (a < 3 and t < 3) else 0.0
+            if mu < 3:
+                K = lower_kappa(mu, CF)
+                words = {"up": (uf, vb), "lo": (KAPPA[K] * uf, KAPPA[K ^ 1] * vb)}
+            else:
+                words = {"up": (uf if CF > 0 else 0.0, vb if CF < 0 else 0.0),
+                         "lo": (uf if CF < 0 else 0.0, vb if CF > 0 else 0.0)}
+            words["lo_neg"] = (-words["lo"][0], -words["lo"][1])
+            for k, (ef, eb) in words.items():
+                for e, row0 in ((ef, 2 * t), (eb, 2 * t + 8)):
+                    lo, hi = bword(complex(e), imc)
+                    B[k][row0, g] = lo
+                    B[k][row0 + 1, g] = hi
+        tiles = {0: (0, "up"), 1: (1, "up")}
+        if mu == 0:
+            tiles.update({2: (1, "lo"), 3: (0, "lo")})
+        elif mu == 1:
+            tiles.update({2: (1, "lo"), 3: (0, "lo_neg")})
+        else:
+            tiles.update({2: (0, "lo"), 3: (1, "lo")})
+        for s, (j, k) in tiles.items():
+            Dt = A[j] @ B[k]
             for lane in range(32):
                 g, t = lane >> 2, lane & 3
-                D[j, lane] += [Dt[g, 2 * t], Dt[g, 2 * t + 1], Dt[g + 8, 2 * t], Dt[g + 8, 2 * t + 1]]
-    out = np.zeros((8, 4, 3), dtype=complex)
+                D[s, lane] += [Dt[g, 2 * t], Dt[g, 2 * t + 1], Dt[g + 8, 2 * t], Dt[g + 8, 2 * t + 1]]
+    out = np.zeros((NR, 4, 3), dtype=complex)
     for lane in range(32):
         g, t = lane >> 2, lane & 3
         if t == 3:
             assert np.all(D[:, lane] == 0)  # the pad column
             continue
-        for j in range(2):
-            out[g, 2 * j, t] = m[g] * complex(D[j, lane, 0], D[j, lane, 1])
-            out[g, 2 * j + 1, t] = m[g] * complex(D[j, lane, 2], D[j, lane, 3])
+        for s in range(4):
+            out[g, s, t] = m[g] * complex(D[s, lane, 0], D[s, lane, 1])
+            out[g + 8, s, t] = m[g + 8] * complex(D[s, lane, 2], D[s, lane, 3])
     np.testing.assert_allclose(out, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
     assert np.all(out[~act] == 0)
 
 
 def test_smem_and_grid_bounds():
-    """Shared memory per block and the partial-sum count the engine allocates."""
-    link_slot, sites, hops = 72, 32, 8  # 4 warps x 8 sites
-    smem = sites * hops * link_slot + sites * hops * 4 + sites * 4 + 4 * 8 * 8  # links, nb, ok, sred
-    assert smem <= 48 * 1024  # static shared memory limit
+    """Dynamic shared memory per block (MmaSmem) and the partial-sum count the engine allocates."""
+    slot = 8 * 3 * 16 * 16 + 8 * 16 * 4  # chunks, norms
+    warp = 2 * slot + 8 * 8 * 9 * 4 + 8 * 8 * 4 + 8 * 4  # two slots, links, nb, ok
+    smem = 4 * warp + 4 * 16 * 8  # + sred
+    assert smem % 16 == 0 and warp % 16 == 0
+    assert 3 * smem <= 228 * 1024  # three resident blocks per SM
     for vh in (4 * 6 * 4 * 8 // 2, 24 ** 3 * 48 // 2, 16 ** 3 * 32 // 2, 7):
-        nblk = -(-vh // sites) * 2  # both parities
+        nblk = -(-vh // 32) * 2  # 32 sites per block, both parities
         assert nblk <= vh + 64
+
+
+def test_fetch_covers_every_chunk_once():
+    """mma_fetch: lane L copies RHS L % 16 of hops 4 (L // 16) .. + 3, every colour, and their norms."""
+    seen, norms = set(), set()
+    for lane in range(32):
+        r, h = lane & 15, lane >> 4
+        for k in range(4):
+            q = 4 * h + k
+            for t in range(3):
+                seen.add((q, t, r ^ (2 * t)))
+            norms.add((r, q))  # S.norm[r][q]: a lane reads its RHS's eight norms as two 16-byte words
+    assert len(seen) == 8 * 3 * 16 and len(norms) == 8 * 16
