@@ -369,6 +369,9 @@ def run_ours(args):
         eng.close()
         serve = run_serving(args, dev)
 
+    # ---- HMC (config C4 couplings on 16^3x32): seconds per trajectory and CG iterations
+    hmc = run_hmc_leg(args) if args.hmc_traj > 0 else None
+
     # ---- CPU baseline (rank 0, N=1): C restatement of the reference's FP64 CG
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -404,6 +407,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "serve": serve,
+            "hmc": hmc,
             # kept last, so that a tail of the line still holds them
             "dslash": dslash_native,
             "dslash_fp64_reference_layout": dslash,
@@ -418,6 +422,32 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_hmc_leg(args):
+    """Nf=2 HMC with the C4 couplings (16^3x32, beta 5.6, kappa 0.150, MinNorm2 nmd 10, tau 1,
+    start exp(i 0.1 H), FP32 force solves at 1e-8 with FP64 reliable updates, FP64 Hamiltonian
+    solves at 1e-10) through the drop-in theory and HMC driver: one untimed trajectory, then
+    `--hmc-traj` timed ones (wall clock around each, synchronised).  From this start every
+    trajectory is rejected (dH ~ 900), which does not change its cost."""
+    import contextlib
+    import io
+
+    from jaxqft_b200 import hmc_run
+
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):  # keep bench's stdout to its one JSON line
+        summ = hmc_run.main(["--shape", "16,16,16,32", "--ntraj", str(args.hmc_traj + 1), "--precision", "single"])
+    recs = [json.loads(l) for l in buf.getvalue().splitlines() if l.startswith('{"traj"')][1:]
+    secs = [r["seconds"] for r in recs]
+    iters = [r["cg_iters_total"] for r in recs]
+    return {"workload": "C4 HMC trajectory, 16x16x16x32, beta 5.6, kappa 0.150, MinNorm2 nmd 10 tau 1, "
+                        "FP32 force solves (FP64 reliable updates) at 1e-8, FP64 Hamiltonian",
+            "trajectories": len(recs), "s_per_traj": float(np.mean(secs)),
+            "solves_per_traj": float(np.mean([r["solves"] for r in recs])),
+            "cg_iters_per_traj": float(np.mean(iters)),
+            "us_per_cg_iter": float(np.sum(secs) / max(1, np.sum(iters)) * 1e6),
+            "acceptance": summ["acceptance"]}
 
 
 SERVE_VOLUMES = [(8, 8, 8, 8), (12, 12, 12, 24), (16, 16, 16, 32), (24, 24, 24, 48)]
@@ -639,6 +669,7 @@ def main():
     ap.add_argument("--serve-rate2", type=float, default=12.0,
                     help="serving leg: a mean rate one B200 sustains without queue growth")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--hmc-traj", type=int, default=2, help="HMC leg: timed C4 trajectories on 16^3x32 (0: off)")
     ap.add_argument("--fp64-all", action="store_true", help="time plain FP64 CG on all 16 RHS (default 4)")
     ap.add_argument("--profile-iters", type=int, default=0,
                     help="profiling driver: run this many CG iterations between cudaProfilerStart/Stop")

@@ -265,6 +265,16 @@ static bool half_acc_enabled() {
   return on;
 }
 
+// The drop-in pair kernel reads neighbour spinors as 64-byte pieces, one 32-byte sector per
+// thread, and swaps spins within the pair by shuffles (WL_REF_SECTOR=0: per-spin loads).
+static bool ref_sector_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("WL_REF_SECTOR");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 static bool fast_hop_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("WL_FAST_HOP");
@@ -781,7 +791,8 @@ static bool site_hop(wl_ctx* ctx, wl_gauge* G, const void* in, void* out, const 
   const long long n = (parity < 0 ? g.V : g.Vh) * 2LL;  // two threads per target site
   const dim3 grid((unsigned)((n + kRefSiteBlock - 1) / kRefSiteBlock), nrhs);
   g_launches++;
-  if (w32) ref_pair_kernel<DAG, 4><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
+  if (w32 && ref_sector_enabled()) ref_pair_kernel<DAG, 4, true><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
+  else if (w32) ref_pair_kernel<DAG, 4><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
   else ref_pair_kernel<DAG, 2><<<grid, kRefSiteBlock, 0, ctx->stream>>>(A);
   return true;
 }

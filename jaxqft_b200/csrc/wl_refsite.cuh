@@ -136,11 +136,111 @@ WL_D void pair_combine(const double (&a)[6], const double (&b)[6], double sg, cp
   }
 }
 
-template <int MU, int C, int W>
-WL_D void refpair_project(const double* site, int j, double sg, cplx<double> (&h)[3]) {
+// Sector loads (SECT): the pair reads a neighbour's 192 bytes as three 64-byte pieces, one
+// 32-byte sector per thread per instruction, each piece inside one 128-byte line (the site is
+// 64-byte aligned), so an instruction touches one line per site instead of one or two per
+// spin.  Sector k holds complex values z[2k], z[2k+1] (z[3 spin + colour]); thread j takes
+// the sector of each piece that holds more of its own spins and the pair swaps the rest with
+// xor-shuffles (mask pm: the active pairs of the warp):
+//   mu = 0, 1 (spins j, 3 - j): pieces (0,1) (3,2) (5,4); 0 <- z2, z9 of thread 1; 1 <- z6, z7
+//   mu = 2 (spins j, 2 + j): pieces (0,1) (3,2) (4,5); 0 <- z2, 1 <- z9
+//   mu = 3, C > 0 (spin j): pieces (0,1) (3,2); 0 <- z2
+//   mu = 3, C < 0 (spin 2 + j): pieces (3,2) (4,5); 1 <- z9
+// (piece (x, y): thread 0 loads sector x, thread 1 sector y).
+WL_D void ld_sector(const double* site, int sec, double (&v)[4]) { ld_vec<4>(site + 4 * sec, v); }
+
+WL_D double pick(int j, double x0, double x1) { return j ? x1 : x0; }
+
+template <int MU, int C>
+WL_D void ld_pair_spins(const double* site, int j, unsigned pm, double (&a)[6], double (&b)[6]) {
+  double r0[4], r1[4], r2[4];
+  if (MU < 3) {
+    ld_sector(site, j, r0);               // (0, 1)
+    ld_sector(site, 3 - j, r1);           // (3, 2)
+    if (MU < 2) ld_sector(site, 5 - j, r2);  // (5, 4)
+    else ld_sector(site, 4 + j, r2);         // (4, 5)
+  } else if (C > 0) {
+    ld_sector(site, j, r0);
+    ld_sector(site, 3 - j, r1);
+  } else {
+    ld_sector(site, 3 - j, r1);
+    ld_sector(site, 4 + j, r2);
+  }
+  if (MU < 2) {
+    // thread 0 sends z6, z7 (r1); thread 1 sends z2 (r0[0..1]) and z9 (r2[2..3])
+    double x[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double snd = j ? (k < 2 ? r0[k] : r2[k]) : r1[k];
+      x[k] = __shfl_xor_sync(pm, snd, 1);
+    }
+    // a: spin j (t0: z0 z1 z2 = r0[0..3], x[0..1]; t1: z3 z4 z5 = r0[2..3], r1[0..3])
+    // b: spin 3 - j (t0: z9 z10 z11 = x[2..3], r2[0..3]; t1: z6 z7 z8 = x[0..3], r2[0..1])
+    a[0] = pick(j, r0[0], r0[2]);
+    a[1] = pick(j, r0[1], r0[3]);
+    a[2] = pick(j, r0[2], r1[0]);
+    a[3] = pick(j, r0[3], r1[1]);
+    a[4] = pick(j, x[0], r1[2]);
+    a[5] = pick(j, x[1], r1[3]);
+    b[0] = pick(j, x[2], x[0]);
+    b[1] = pick(j, x[3], x[1]);
+    b[2] = pick(j, r2[0], x[2]);
+    b[3] = pick(j, r2[1], x[3]);
+    b[4] = pick(j, r2[2], r2[0]);
+    b[5] = pick(j, r2[3], r2[1]);
+  } else if (MU == 2) {
+    // thread 0 sends z9 (r2[2..3]); thread 1 sends z2 (r0[0..1])
+    double x[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) x[k] = __shfl_xor_sync(pm, j ? r0[k] : r2[2 + k], 1);
+    // a: spin j (t0: z0 z1 z2 = r0, x; t1: z3 z4 z5 = r0[2..3], r1)
+    // b: spin 2 + j (t0: z6 z7 z8 = r1, r2[0..1]; t1: z9 z10 z11 = x, r2)
+    a[0] = pick(j, r0[0], r0[2]);
+    a[1] = pick(j, r0[1], r0[3]);
+    a[2] = pick(j, r0[2], r1[0]);
+    a[3] = pick(j, r0[3], r1[1]);
+    a[4] = pick(j, x[0], r1[2]);
+    a[5] = pick(j, x[1], r1[3]);
+    b[0] = pick(j, r1[0], x[0]);
+    b[1] = pick(j, r1[1], x[1]);
+    b[2] = pick(j, r1[2], r2[0]);
+    b[3] = pick(j, r1[3], r2[1]);
+    b[4] = pick(j, r2[0], r2[2]);
+    b[5] = pick(j, r2[1], r2[3]);
+  } else if (C > 0) {
+    // thread 0 receives z2 (thread 1's r0[0..1]); a = spin j
+    double x[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) x[k] = __shfl_xor_sync(pm, r0[k], 1);
+    a[0] = pick(j, r0[0], r0[2]);
+    a[1] = pick(j, r0[1], r0[3]);
+    a[2] = pick(j, r0[2], r1[0]);
+    a[3] = pick(j, r0[3], r1[1]);
+    a[4] = pick(j, x[0], r1[2]);
+    a[5] = pick(j, x[1], r1[3]);
+  } else {
+    // thread 1 receives z9 (thread 0's r2[2..3]); a = spin 2 + j
+    double x[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) x[k] = __shfl_xor_sync(pm, r2[2 + k], 1);
+    a[0] = pick(j, r1[0], x[0]);
+    a[1] = pick(j, r1[1], x[1]);
+    a[2] = pick(j, r1[2], r2[0]);
+    a[3] = pick(j, r1[3], r2[1]);
+    a[4] = pick(j, r2[0], r2[2]);
+    a[5] = pick(j, r2[1], r2[3]);
+  }
+}
+
+template <int MU, int C, int W, bool SECT>
+WL_D void refpair_project(const double* site, int j, double sg, unsigned pm, cplx<double> (&h)[3]) {
   double a[6], b[6];
-  ld_spin<W>(site, pair_spin1<MU, C>(j), a);
-  if (MU < 3) ld_spin<W>(site, pair_spin2<MU>(j), b);
+  if (SECT) {
+    ld_pair_spins<MU, C>(site, j, pm, a, b);
+  } else {
+    ld_spin<W>(site, pair_spin1<MU, C>(j), a);
+    if (MU < 3) ld_spin<W>(site, pair_spin2<MU>(j), b);
+  }
   pair_combine<MU, C>(a, b, sg, h);
 }
 
@@ -195,6 +295,58 @@ WL_D void pair_store(const RefSiteArgs& A, size_t off, bool act, int j, const cp
   for (int k = 0; k < 12; k += W) st_vec<W>(A.out + off + k, o + k);
 }
 
+// Sector form of pair_store: after the assembly thread j holds sectors 3j..3j+2 of the site
+// (its two spins); one more shuffle swaps sector 1 (thread 0) with sector 4 (thread 1), so
+// thread j writes sectors j, 2 + j, 4 + j and every store instruction of the pair covers one
+// 64-byte piece, as the loads do; the self term is read in the same pieces.  `site` is the
+// site's first double.  Every lane must call it.
+WL_D void pair_store_sect(const RefSiteArgs& A, size_t site, bool act, int j, const cplx<double> (&Ac)[3],
+                          const cplx<double> (&Xc)[3], const cplx<double> (&Yc)[3]) {
+  cplx<double> lo[3], hi[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const cplx<double> r1 = shfl_pair(j == 0 ? Xc[a] : Ac[a]);
+    const cplx<double> r2 = shfl_pair(Yc[a]);
+    if (j == 0) {
+      lo[a] = Ac[a];
+      hi[a] = r1;
+    } else {
+      lo[a] = r2 + Xc[a];
+      hi[a] = r1 + Yc[a];
+    }
+  }
+  double o[12];  // sectors 3j, 3j + 1, 3j + 2 of b * acc
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    o[2 * a] = A.b * lo[a].re;
+    o[2 * a + 1] = A.b * lo[a].im;
+    o[6 + 2 * a] = A.b * hi[a].re;
+    o[6 + 2 * a + 1] = A.b * hi[a].im;
+  }
+#pragma unroll
+  for (int k = 4; k < 8; ++k) o[k] = __shfl_xor_sync(0xffffffffu, o[k], 1);  // sector 1 <-> sector 4
+  if (!act) return;
+  // this thread's sectors j, 2 + j, 4 + j, in that order
+  double v[12];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = j ? o[4 + k] : o[k];
+    v[4 + k] = j ? o[k] : o[8 + k];
+    v[8 + k] = j ? o[8 + k] : o[4 + k];
+  }
+  if (A.self) {
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      double x[4];
+      ld_vec<4>(A.self + site + 8 * p + 4 * j, x);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[4 * p + k] = fma(A.a, x[k], v[4 * p + k]);
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 3; ++p) st_vec<4>(A.out + site + 8 * p + 4 * j, v + 4 * p);
+}
+
 // site coordinates of flat index f
 WL_D Site site_of_flat(const Geom& g, int f) {
   Site s;
@@ -211,9 +363,9 @@ WL_D Site site_of_flat(const Geom& g, int f) {
   return s;
 }
 
-template <int MU, bool DAG, int W>
+template <int MU, bool DAG, int W, bool SECT>
 WL_D void refpair_mu(const RefSiteArgs& A, const double* base, const Site& s, int parity, int j, double sg,
-                     cplx<double> (&Ac)[3], cplx<double> (&Xc)[3], cplx<double> (&Yc)[3]) {
+                     unsigned pm, cplx<double> (&Ac)[3], cplx<double> (&Xc)[3], cplx<double> (&Yc)[3]) {
   constexpr int CF = DAG ? +1 : -1;
   constexpr int CB = -CF;
   const Geom& g = A.g;
@@ -229,10 +381,10 @@ WL_D void refpair_mu(const RefSiteArgs& A, const double* base, const Site& s, in
     else ld_link(A.U, vh, 1 - parity, MU, nb, u);
     cplx<double> h[3];
     if (dir == 0) {
-      refpair_project<MU, CF, W>(src, j, sg, h);
+      refpair_project<MU, CF, W, SECT>(src, j, sg, pm, h);
       pair_hop<MU, CF, false>(u, h, g.ph_on[MU] && s.x[MU] == g.L[MU] - 1, g, sg, Ac, Xc, Yc);
     } else {
-      refpair_project<MU, CB, W>(src, j, sg, h);
+      refpair_project<MU, CB, W, SECT>(src, j, sg, pm, h);
       pair_hop<MU, CB, true>(u, h, g.ph_on[MU] && s.x[MU] == 0, g, sg, Ac, Xc, Yc);
     }
   }
@@ -242,8 +394,9 @@ WL_D void refpair_mu(const RefSiteArgs& A, const double* base, const Site& s, in
 #define WL_REFPAIR_MINB 4  // resident 128-thread blocks per SM the pair kernel is compiled for
 #endif
 
-template <bool DAG, int W>
+template <bool DAG, int W, bool SECT = false>
 __global__ void __launch_bounds__(kRefSiteBlock, WL_REFPAIR_MINB) ref_pair_kernel(RefSiteArgs A) {
+  static_assert(!SECT || W == 4, "sector loads use 32-byte vectors");
   const Geom& g = A.g;
   const int i = blockIdx.x * (blockDim.x >> 1) + (threadIdx.x >> 1);
   const int j = threadIdx.x & 1;
@@ -256,6 +409,7 @@ __global__ void __launch_bounds__(kRefSiteBlock, WL_REFPAIR_MINB) ref_pair_kerne
 #pragma unroll
   for (int a = 0; a < 3; ++a) Ac[a] = Xc[a] = Yc[a] = {0.0, 0.0};
   const size_t field = (size_t)rhs * g.V * 24;
+  const unsigned pm = __ballot_sync(0xffffffffu, act);  // both threads of a pair share `act`
   if (act) {
     if (A.parity < 0) {  // every site: i is the flat index
       s = site_of_flat(g, i);
@@ -265,13 +419,14 @@ __global__ void __launch_bounds__(kRefSiteBlock, WL_REFPAIR_MINB) ref_pair_kerne
       s = site_from_compact(g, parity, i);
     }
     const double* base = A.in + field;
-    refpair_mu<0, DAG, W>(A, base, s, parity, j, sg, Ac, Xc, Yc);
-    refpair_mu<1, DAG, W>(A, base, s, parity, j, sg, Ac, Xc, Yc);
-    refpair_mu<2, DAG, W>(A, base, s, parity, j, sg, Ac, Xc, Yc);
-    refpair_mu<3, DAG, W>(A, base, s, parity, j, sg, Ac, Xc, Yc);
+    refpair_mu<0, DAG, W, SECT>(A, base, s, parity, j, sg, pm, Ac, Xc, Yc);
+    refpair_mu<1, DAG, W, SECT>(A, base, s, parity, j, sg, pm, Ac, Xc, Yc);
+    refpair_mu<2, DAG, W, SECT>(A, base, s, parity, j, sg, pm, Ac, Xc, Yc);
+    refpair_mu<3, DAG, W, SECT>(A, base, s, parity, j, sg, pm, Ac, Xc, Yc);
   }
   const size_t flat = (size_t)s.row * g.L[3] + s.x[3];
-  pair_store<W>(A, field + flat * 24 + 12 * j, act, j, Ac, Xc, Yc);  // this thread's two spins
+  if (SECT) pair_store_sect(A, field + flat * 24, act, j, Ac, Xc, Yc);
+  else pair_store<W>(A, field + flat * 24 + 12 * j, act, j, Ac, Xc, Yc);  // this thread's two spins
 }
 
 }  // namespace wl
