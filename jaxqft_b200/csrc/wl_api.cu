@@ -217,7 +217,7 @@ static SpinorRef sref(const void* p, const Geom& g) {
 struct Tune {
   int nr = 1, bx = 128, by = 1;
   int lanes = 0;  // > 0: RHS-in-lanes hop (FP16/FP32 storage) with this many RHS lanes per site
-  int pair = 0;   // 1: FP64 single-RHS stencil with two threads per site (hop_pair_kernel)
+  int pair = 0;   // 1: single-RHS stencil with two threads per site (hop_pair_kernel; FP64 or FP32 storage)
   int seq = 1;    // FP64 RHS-in-lanes hop: groups of `lanes` RHS each block works through in turn
   // 1: FP16 hop on the tensor cores (hop_mma_kernel, 16 RHS per warp) where its epilogue
   // allows.  Selected only by WL_FORCE_TUNE: at 24^3x48 with 16 RHS it takes 0.45 ms per hop
@@ -307,12 +307,7 @@ template <bool DAG, class IDX, class LF, class SF, class EPI>
 static void launch_hop(const Tune& t0, const HopArgs<LF, SF, EPI>& a, int npar, cudaStream_t st) {
   const Tune t = effective_tune<IDX, SF, EPI>(t0);
   launch_hop_impl<DAG, IDX>(t, a, npar, st);
-  if (EPI::kReduce) {
-    const bool lanes = (UsesFastHop<SF>::value || std::is_same<SF, SpinorField<P_DOUBLE>>::value) &&
-                       std::is_same<IDX, IdxCompact>::value && t.lanes > 0;
-    (void)lanes;  // lane kernels also write one partial per block
-    launch_finalize(a.red, a.nrhs, grid_for(a.g, t, a.nrhs, npar), a.mask, st, 1);
-  }
+  if (EPI::kReduce) launch_finalize(a.red, a.nrhs, grid_for(a.g, t, a.nrhs, npar), a.mask, st, 1);
 }
 
 template <bool DAG, class IDX, class LF, class SF, class EPI>
@@ -333,6 +328,13 @@ static void launch_hop_impl(const Tune& t, const HopArgs<LF, SF, EPI>& a, int np
       return;
     }
     if (t.pair) {
+      hop_pair_kernel<DAG><<<grid, dim3(t.bx, 1, 1), 0, st>>>(a);
+      return;
+    }
+  }
+  if constexpr (std::is_same<SF, SpinorField<P_SINGLE>>::value && std::is_same<IDX, IdxCompact>::value &&
+                std::is_same<typename LF::real, float>::value) {
+    if (t.pair && t.lanes == 0) {
       hop_pair_kernel<DAG><<<grid, dim3(t.bx, 1, 1), 0, st>>>(a);
       return;
     }
@@ -1156,6 +1158,13 @@ struct wl_engine {
   cudaGraphConditionalHandle cond = 0;
   int* ru_iters = nullptr;         // device: iterations whose conditional body ran
   long long ru_iters_seen = 0;
+  // the solve as one graph (WHILE node over the iteration), launched once per wl_solve
+  cudaGraphExec_t gloop = nullptr;
+  int* loop_count = nullptr;       // device: iterations run by the loop graph's current launch
+  long long loop_kernels = 0;      // unconditional kernels per loop iteration
+  int loop_cap = 0;                // maxiter the loop graph was built for
+  unsigned long long loop_gauge_id = 0;
+  bool loop_failed = false;        // the loop graph could not be built: host-driven loop
   bool ru_links12 = false;         // FP64 true residual with 12-real links (links unitary to 1e-12)
 };
 
@@ -1674,7 +1683,7 @@ static Tune autotune_hop(wl_engine* E, cudaStream_t st) {
         cands.push_back(Tune{nr, bx, by});
       }
   }
-  if (S == P_DOUBLE && !E->lanes_mode)
+  if ((S == P_DOUBLE || S == P_SINGLE) && !E->lanes_mode)
     for (int bx : {64, 128, 256}) {
       Tune t;
       t.bx = bx;
@@ -1802,7 +1811,7 @@ static Tune pick_tune(wl_engine* E, cudaStream_t st) {
         if (t.lanes > 0 && !E->lanes_mode) t = Tune{};  // FP64 iteration or < 4 slots: thread-per-site kernel
         if (t.mma && (t.lanes == 0 || E->sprec != P_HALF)) t.mma = 0;  // FP16 lanes engines only
         if (t.lanes > 0) t.bx = kLaneBlock;
-        if (t.pair && (E->sprec != P_DOUBLE || E->lanes_mode || t.lanes > 0)) t.pair = 0;  // FP64 sites only
+        if (t.pair && (E->sprec == P_HALF || E->lanes_mode || t.lanes > 0)) t.pair = 0;  // FP64 / FP32 sites only
         if (t.pair) t.nr = 1, t.by = 1;
         return t;
       }
@@ -1844,6 +1853,7 @@ extern "C" void wl_engine_destroy(wl_engine* E) {
   cudaStream_t st = engine_stream(E);
   if (st) cudaStreamSynchronize(st);
   if (E->gexec) cudaGraphExecDestroy(E->gexec);
+  if (E->gloop) cudaGraphExecDestroy(E->gloop);
   IField* fs[] = {&E->b64, &E->x64, &E->y64, &E->t64, &E->xs, &E->rs, &E->p, &E->y, &E->t1};
   for (IField* f : fs) free_field(*f);
   cudaFree(E->dbl);
@@ -1851,6 +1861,7 @@ extern "C" void wl_engine_destroy(wl_engine* E) {
   cudaFree(E->partials);
   cudaFree(E->counters);
   cudaFree(E->ru_iters);
+  cudaFree(E->loop_count);
   if (E->h_pinned) cudaFreeHost(E->h_pinned);
   if (E->poll_ev) cudaEventDestroy(E->poll_ev);
   if (st) cudaStreamDestroy(st);
@@ -1936,6 +1947,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   if (e == cudaSuccess) e = cudaMalloc(&E->counters, sizeof(unsigned) * (n + 1));
   if (e == cudaSuccess) e = cudaMallocHost(&E->h_pinned, sizeof(int) * (3 * n + 2));
   if (e == cudaSuccess) e = cudaMalloc(&E->ru_iters, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&E->loop_count, sizeof(int));
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->poll_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     ctx->err = std::string("engine allocation: ") + cudaGetErrorString(e);
@@ -2035,70 +2047,81 @@ static wl_status engine_admit_all(wl_engine* E, const void* b, const void* x0, c
   return admit_impl(E, slots.data(), n, b, x0, masses, nullptr, nullptr);
 }
 
-static wl_status build_graph(wl_engine* E, cudaStream_t st) {
-  wl_ctx* ctx = E->ctx;
+// Appends one CG iteration to graph `g` (captured from stream st): part 1, the reliable-update
+// body (part 2) inside an IF node on a conditional handle created on g (the decide kernel of
+// part 1 sets it), then part 3 and, with `loop` set, the kernel that drives an enclosing WHILE
+// node.  Counts the unconditional kernels in *uncond and the body's in E->ru_body_kernels.
+static cudaError_t capture_iteration(wl_engine* E, cudaStream_t st, cudaGraph_t g, const SolveLoop* loop,
+                                     long long* uncond) {
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
-  cudaGraph_t graph = nullptr;
-  WL_CUDA(ctx, cudaGraphCreate(&graph, 0));
-  cudaError_t e = cudaGraphConditionalHandleCreate(&E->cond, graph, 0, cudaGraphCondAssignDefault);
-  if (e != cudaSuccess) {
-    cudaGraphDestroy(graph);
-    ctx->err = std::string("cudaGraphConditionalHandleCreate: ") + cudaGetErrorString(e);
-    return WL_ERR_CUDA;
-  }
+  cudaGraphConditionalHandle cond = 0;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return e;
+  E->cond = cond;  // captured by value into the decide kernel of this iteration
   E->use_cond = true;
   const long long before = g_launches.load();
-  // part 1: sloppy operator, CG update, reliable-update decision
-  e = cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, mode);
+  e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, mode);
+  if (e != cudaSuccess) return e;
+  enqueue_part(E, st, 1);
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  std::vector<cudaGraphNode_t> dv;
+  e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
+  if (e == cudaSuccess) dv.assign(deps, deps + ndeps);
+  cudaGraph_t g1 = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(st, &g1);
+  if (e == cudaSuccess) e = e2;
+  long long n_uncond = g_launches.load() - before;
+  cudaGraphNode_t cond_node = nullptr;
   if (e == cudaSuccess) {
-    enqueue_part(E, st, 1);
-    cudaStreamCaptureStatus cs;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    std::vector<cudaGraphNode_t> dv;
-    e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
-    if (e == cudaSuccess) dv.assign(deps, deps + ndeps);
-    cudaGraph_t g1 = nullptr;
-    cudaError_t e2 = cudaStreamEndCapture(st, &g1);
-    if (e == cudaSuccess) e = e2;
-    const long long part13 = g_launches.load();
-    // part 2 in a conditional IF node
-    cudaGraphNode_t cond_node = nullptr;
+    // cudaGraphNodeParams has no default constructor (it holds a union): zeroed storage
+    alignas(cudaGraphNodeParams) unsigned char cpbuf[sizeof(cudaGraphNodeParams)];
+    std::memset(cpbuf, 0, sizeof(cpbuf));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cpbuf);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&cond_node, g, dv.data(), dv.size(), &cp);
     if (e == cudaSuccess) {
-      // cudaGraphNodeParams has no default constructor (it holds a union): zeroed storage
-      alignas(cudaGraphNodeParams) unsigned char cpbuf[sizeof(cudaGraphNodeParams)];
-      std::memset(cpbuf, 0, sizeof(cpbuf));
-      cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cpbuf);
-      cp.type = cudaGraphNodeTypeConditional;
-      cp.conditional.handle = E->cond;
-      cp.conditional.type = cudaGraphCondTypeIf;
-      cp.conditional.size = 1;
-      e = cudaGraphAddNode(&cond_node, graph, dv.data(), dv.size(), &cp);
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, mode);
       if (e == cudaSuccess) {
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, mode);
-        if (e == cudaSuccess) {
-          const long long b0 = g_launches.load();
-          enqueue_part(E, st, 2);
-          E->ru_body_kernels = g_launches.load() - b0;
-          cudaGraph_t gb = nullptr;
-          e = cudaStreamEndCapture(st, &gb);
-        }
+        const long long b0 = g_launches.load();
+        enqueue_part(E, st, 2);
+        E->ru_body_kernels = g_launches.load() - b0;
+        cudaGraph_t gb = nullptr;
+        e = cudaStreamEndCapture(st, &gb);
       }
     }
-    // part 3 after the conditional node
+  }
+  if (e == cudaSuccess) {
+    e = cudaStreamBeginCaptureToGraph(st, g, &cond_node, nullptr, 1, mode);
     if (e == cudaSuccess) {
       const long long p3 = g_launches.load();
-      e = cudaStreamBeginCaptureToGraph(st, graph, &cond_node, nullptr, 1, mode);
-      if (e == cudaSuccess) {
-        enqueue_part(E, st, 3);
-        cudaGraph_t g3 = nullptr;
-        e = cudaStreamEndCapture(st, &g3);
+      enqueue_part(E, st, 3);
+      if (loop) {
+        g_launches++;
+        solve_loop_kernel<<<1, 1, 0, st>>>(*loop);
       }
-      E->graph_kernels = (part13 - before) + (g_launches.load() - p3);
+      n_uncond += g_launches.load() - p3;
+      cudaGraph_t g3 = nullptr;
+      e = cudaStreamEndCapture(st, &g3);
     }
   }
   g_launches = before;  // captured, not launched
+  *uncond = n_uncond;
+  return e;
+}
+
+static wl_status build_graph(wl_engine* E, cudaStream_t st) {
+  wl_ctx* ctx = E->ctx;
+  cudaGraph_t graph = nullptr;
+  WL_CUDA(ctx, cudaGraphCreate(&graph, 0));
+  long long nk = 0;
+  cudaError_t e = capture_iteration(E, st, graph, nullptr, &nk);
+  E->graph_kernels = nk;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&E->gexec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) {
@@ -2108,6 +2131,52 @@ static wl_status build_graph(wl_engine* E, cudaStream_t st) {
     return WL_ERR_CUDA;
   }
   E->graph_built = true;
+  return WL_OK;
+}
+
+// The whole solve as one graph: a WHILE node whose body is one iteration followed by
+// solve_loop_kernel, which keeps the loop going while any slot is active and fewer than
+// `cap` iterations have run (a hard bound on the device loop; slots stop at their maxiter
+// long before).  wl_solve launches it once per solve instead of launching an iteration graph
+// and synchronising on a status poll every check_every iterations.  On any failure the
+// engine keeps the host-driven loop.
+static wl_status build_loop_graph(wl_engine* E, cudaStream_t st) {
+  wl_ctx* ctx = E->ctx;
+  cudaGraph_t graph = nullptr;
+  WL_CUDA(ctx, cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle wh = 0;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&wh, graph, 1, cudaGraphCondAssignDefault);
+  cudaGraphNode_t wnode = nullptr;
+  cudaGraph_t body = nullptr;
+  if (e == cudaSuccess) {
+    alignas(cudaGraphNodeParams) unsigned char cpbuf[sizeof(cudaGraphNodeParams)];
+    std::memset(cpbuf, 0, sizeof(cpbuf));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cpbuf);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = wh;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&wnode, graph, nullptr, 0, &cp);
+    if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
+  }
+  long long nk = 0;
+  if (e == cudaSuccess) {
+    int cap = 0;
+    for (int m : E->h_maxiter) cap = std::max(cap, m);
+    SolveLoop L{E->n_active, E->loop_count, cap + 8, wh};
+    e = capture_iteration(E, st, body, &L, &nk);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&E->gloop, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    E->gloop = nullptr;
+    E->loop_failed = true;
+    cudaGetLastError();
+    return WL_ERR_CUDA;
+  }
+  E->loop_kernels = nk;
+  E->loop_cap = 0;
+  for (int m : E->h_maxiter) E->loop_cap = std::max(E->loop_cap, m);
   return WL_OK;
 }
 
@@ -2336,6 +2405,37 @@ extern "C" wl_status wl_engine_retire(wl_engine* E, int slot, void* x, wl_solve_
 }
 
 // ------------------------------------------------------------------ solve
+// One launch of the engine's whole-solve graph (built on first use, rebuilt when the gauge or
+// the iteration limit changed); *ran is false when the graph is unavailable and the caller
+// drives the iterations from the host instead.
+static wl_status run_loop_graph(wl_engine* E, bool* ran) {
+  *ran = false;
+  if (E->loop_failed) return WL_OK;
+  wl_ctx* ctx = E->ctx;
+  cudaStream_t st = engine_stream(E);
+  int cap = 0;
+  for (int m : E->h_maxiter) cap = std::max(cap, m);
+  if (E->gloop && (E->loop_gauge_id != E->gauge->id || E->loop_cap != cap)) {
+    cudaGraphExecDestroy(E->gloop);
+    E->gloop = nullptr;
+  }
+  if (!E->gloop) {
+    if (build_loop_graph(E, st) != WL_OK) {
+      ctx->err.clear();
+      return WL_OK;
+    }
+    E->loop_gauge_id = E->gauge->id;
+  }
+  const int n = E->n;
+  WL_CUDA(ctx, cudaMemsetAsync(E->loop_count, 0, sizeof(int), st));
+  WL_CUDA(ctx, cudaGraphLaunch(E->gloop, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned + 2 + n, E->loop_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+  WL_CUDA(ctx, cudaStreamSynchronize(st));
+  g_launches += (long long)E->h_pinned[2 + n] * E->loop_kernels;
+  *ran = true;
+  return WL_OK;
+}
+
 struct SolveKey {
   const wl_ctx* ctx;
   int op, prec, n, graph;
@@ -2375,6 +2475,10 @@ extern "C" wl_status wl_solve(wl_ctx* ctx, wl_gauge* G, const wl_solve_params* p
       E->gexec = nullptr;
       E->graph_built = false;
     }
+    if (E->gloop && delta_changed) {
+      cudaGraphExecDestroy(E->gloop);
+      E->gloop = nullptr;
+    }
   } else {
     wl_status s = wl_engine_create(ctx, G, prm, nrhs, &E);
     if (s != WL_OK) return s;
@@ -2383,7 +2487,10 @@ extern "C" wl_status wl_solve(wl_ctx* ctx, wl_gauge* G, const wl_solve_params* p
   int n_active = 1;
   long long done_iters = 0;
   const int chunk = E->prm.check_every;
-  while (s == WL_OK) {
+  bool looped = false;
+  if (s == WL_OK && E->prm.use_graph) s = run_loop_graph(E, &looped);
+  if (looped) s = wl_engine_poll(E, nullptr, &n_active);  // status, counters, wait errors
+  while (s == WL_OK && !looped) {
     s = wl_engine_poll(E, nullptr, &n_active);
     if (s != WL_OK || n_active == 0) break;
     if (done_iters > (long long)E->prm.maxiter + 2 * chunk) break;  // host-side guard

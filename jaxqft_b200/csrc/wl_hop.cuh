@@ -171,7 +171,11 @@ WL_D void hop_dir(const Geom& g, const LF& links, const SF& src, int parity, con
 // Launch-wide reductions: every block writes one partial sum per RHS it
 // covers into partials[rhs][block]; reduce_finalize_kernel (launched right
 // after, one block per RHS) adds them in a fixed order.  Deterministic run to
-// run, no floating-point atomics and no per-block fences.
+// run, no floating-point atomics and no per-block fences.  (Finishing the sum
+// in the last block of the launch instead -- a fence, a block counter and one
+// block reading every partial -- was measured slower on the 16^3x32 HMC
+// solves: the fence before each block's count lengthened every hop by more
+// than the finalize launch it saved.)
 struct Reduce {
   double* partials;   // [nrhs][nblk]
   unsigned* counter;  // unused (kept for layout stability)
@@ -285,9 +289,9 @@ __global__ void __launch_bounds__(256) hop_kernel(HopArgs<LF, SF, EPI> A) {
   if (EPI::kReduce) reduce_rhs<NR>(red, A.red, A.nrhs, A.mask);
 }
 
-// ------------------------------------------------------------------ FP64, two threads per site
-// Single-RHS FP64 stencil with a pair of threads per target site.  Thread j
-// (j = lane & 1) forms half-spinor row j of every hop,
+// ------------------------------------------------------------------ one RHS, two threads per site
+// Single-RHS stencil (FP64 or FP32 storage) with a pair of threads per target
+// site.  Thread j (j = lane & 1) forms half-spinor row j of every hop,
 //   mu=0: h = s_j + c s_{3-j}      mu=1: h = s_j + (1-2j) c' s_{3-j}
 //   mu=2: h = s_j + c' s_{2+j}     mu=3: 2 s_j (c = +1) or 2 s_{2+j} (c = -1)
 // (c' = -i c), so it loads only the two spin components it needs; both threads
@@ -296,35 +300,57 @@ __global__ void __launch_bounds__(256) hop_kernel(HopArgs<LF, SF, EPI> A) {
 // and partial sums X of a_{3-j} and Y of a_{2+j}; one xor-shuffle exchange
 // assembles the site in thread 0, which runs the epilogue.  Per thread this
 // holds about half the registers of hop_kernel, so twice as many threads per
-// SM keep neighbour loads in flight.
-template <int MU, int C>
-WL_D void pair_project(const SpinorField<P_DOUBLE>& src, int rhs, unsigned nb, int j, double sg,
-                       cplx<double> (&h)[3]) {
-  const int s1 = (MU == 3 && C < 0) ? 2 + j : j;
-  const int s2 = MU == 2 ? 2 + j : 3 - j;
+// SM keep neighbour loads in flight.  FP64 engines of 1-3 slots use it at
+// 24^3x48; for FP32 storage it is an autotuner candidate (at 16^3x32 with one
+// RHS, an L2-resident working set, the thread-per-site FP32 kernel measured
+// faster: 10.3 against 12.3 us per half-lattice hop).
+
+// Spin s (three colours) of an FP32 record: complex z = 3 s + colour sits in
+// 16-byte chunk z / 2 (half z % 2), so spin s is chunk (3 s - (s & 1)) / 2 from
+// colour 0 (even s: the whole chunk; odd s: its upper half) and the next chunk.
+WL_D void pair_spin_load(const SpinorField<P_SINGLE>& f, int rhs, unsigned c, int s, cplx<float> (&v)[3]) {
+  const int odd = s & 1;
+  const int k0 = (3 * s - odd) >> 1;
+  const float4 q0 = ldg(f.ptr + f.at(rhs, k0, c));
+  const float4 q1 = ldg(f.ptr + f.at(rhs, k0 + 1, c));
+  v[0] = odd ? cplx<float>{q0.z, q0.w} : cplx<float>{q0.x, q0.y};
+  v[1] = odd ? cplx<float>{q1.x, q1.y} : cplx<float>{q0.z, q0.w};
+  v[2] = odd ? cplx<float>{q1.z, q1.w} : cplx<float>{q1.x, q1.y};
+}
+WL_D void pair_spin_load(const SpinorField<P_DOUBLE>& f, int rhs, unsigned c, int s, cplx<double> (&v)[3]) {
 #pragma unroll
   for (int col = 0; col < 3; ++col) {
-    const double2 a = ldg(src.ptr + src.at(rhs, s1 * 3 + col, nb));
+    const double2 a = ldg(f.ptr + f.at(rhs, s * 3 + col, c));
+    v[col] = {a.x, a.y};
+  }
+}
+
+template <int MU, int C, class SF, typename T>
+WL_D void pair_project(const SF& src, int rhs, unsigned nb, int j, T sg, cplx<T> (&h)[3]) {
+  const int s1 = (MU == 3 && C < 0) ? 2 + j : j;
+  const int s2 = MU == 2 ? 2 + j : 3 - j;
+  cplx<T> a[3], b[3];
+  pair_spin_load(src, rhs, nb, s1, a);
+  if (MU < 3) pair_spin_load(src, rhs, nb, s2, b);
+#pragma unroll
+  for (int col = 0; col < 3; ++col) {
     if (MU == 3) {
-      h[col] = {2.0 * a.x, 2.0 * a.y};
+      h[col] = {T(2) * a[col].re, T(2) * a[col].im};
       continue;
     }
-    const double2 b = ldg(src.ptr + src.at(rhs, s2 * 3 + col, nb));
     if (MU == 0) {
-      h[col] = C > 0 ? cplx<double>{a.x + b.x, a.y + b.y} : cplx<double>{a.x - b.x, a.y - b.y};
+      h[col] = C > 0 ? a[col] + b[col] : a[col] - b[col];
     } else {
-      // w = -i C b
-      const cplx<double> w = C > 0 ? mul_mi(cplx<double>{b.x, b.y}) : mul_i(cplx<double>{b.x, b.y});
-      if (MU == 1) h[col] = {fma(sg, w.re, a.x), fma(sg, w.im, a.y)};
-      else h[col] = {a.x + w.re, a.y + w.im};
+      const cplx<T> w = C > 0 ? mul_mi(b[col]) : mul_i(b[col]);  // w = -i C b
+      if (MU == 1) h[col] = {fma(sg, w.re, a[col].re), fma(sg, w.im, a[col].im)};
+      else h[col] = a[col] + w;
     }
   }
 }
 
 // Accumulate colour component a of one hop, uh, into A, X, Y (see above).
-template <int MU, int C>
-WL_D void pair_accum(int a, cplx<double> uh, double sg, cplx<double> (&A)[3], cplx<double> (&X)[3],
-                     cplx<double> (&Y)[3]) {
+template <int MU, int C, typename T>
+WL_D void pair_accum(int a, cplx<T> uh, T sg, cplx<T> (&A)[3], cplx<T> (&X)[3], cplx<T> (&Y)[3]) {
   if (MU == 3) {
     if (C > 0) A[a] = A[a] + uh;
     else Y[a] = Y[a] + uh;
@@ -334,89 +360,101 @@ WL_D void pair_accum(int a, cplx<double> uh, double sg, cplx<double> (&A)[3], cp
   if (MU == 0) {
     X[a] = C > 0 ? X[a] + uh : X[a] - uh;
   } else if (MU == 1) {  // X += (1-2j) (i C) uh
-    const cplx<double> w = C > 0 ? mul_i(uh) : mul_mi(uh);
+    const cplx<T> w = C > 0 ? mul_i(uh) : mul_mi(uh);
     X[a] = {fma(sg, w.re, X[a].re), fma(sg, w.im, X[a].im)};
   } else {  // Y += (i C) uh
     Y[a] = Y[a] + (C > 0 ? mul_i(uh) : mul_mi(uh));
   }
 }
 
-template <int MU, int C, bool DAGU>
-WL_D void pair_hop(const Link<double>& u, const cplx<double> (&h)[3], bool ph, const Geom& g, double sg,
-                   cplx<double> (&A)[3], cplx<double> (&X)[3], cplx<double> (&Y)[3]) {
+template <int MU, int C, bool DAGU, typename T>
+WL_D void pair_hop(const Link<T>& u, const cplx<T> (&h)[3], bool ph, const Geom& g, T sg, cplx<T> (&A)[3],
+                   cplx<T> (&X)[3], cplx<T> (&Y)[3]) {
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    cplx<double> uh = {0.0, 0.0};
+    cplx<T> uh = {T(0), T(0)};
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
       if (DAGU) fmac_(uh, u.m[b][a], h[b]);
       else fma_(uh, u.m[a][b], h[b]);
     }
-    if (ph) uh = uh * cplx<double>{g.ph_re[MU], DAGU ? -g.ph_im[MU] : g.ph_im[MU]};
+    if (ph) uh = uh * cplx<T>{T(g.ph_re[MU]), T(DAGU ? -g.ph_im[MU] : g.ph_im[MU])};
     pair_accum<MU, C>(a, uh, sg, A, X, Y);
   }
 }
 
-template <int MU, bool DAG, class LF>
-WL_D void pair_dir(const Geom& g, const LF& links, const SpinorField<P_DOUBLE>& src, int parity, const Site& s,
-                   int rhs, int j, double sg, cplx<double> (&A)[3], cplx<double> (&X)[3], cplx<double> (&Y)[3]) {
+template <int MU, bool DAG, class LF, class SF, typename T>
+WL_D void pair_dir(const Geom& g, const LF& links, const SF& src, int parity, const Site& s, int rhs, int j, T sg,
+                   cplx<T> (&A)[3], cplx<T> (&X)[3], cplx<T> (&Y)[3]) {
   constexpr int CF = DAG ? +1 : -1;
   constexpr int CB = -CF;
   {
     const unsigned nb = (unsigned)neighbor(g, s, MU, +1);
-    Link<double> u;
+    Link<T> u;
     links.load(u, parity, MU, s.c);
-    cplx<double> h[3];
+    cplx<T> h[3];
     pair_project<MU, CF>(src, rhs, nb, j, sg, h);
     pair_hop<MU, CF, false>(u, h, g.ph_on[MU] && (s.x[MU] == g.L[MU] - 1), g, sg, A, X, Y);
   }
   {
     const unsigned nb = (unsigned)neighbor(g, s, MU, -1);
-    Link<double> u;
+    Link<T> u;
     links.load(u, 1 - parity, MU, (int)nb);
-    cplx<double> h[3];
+    cplx<T> h[3];
     pair_project<MU, CB>(src, rhs, nb, j, sg, h);
     pair_hop<MU, CB, true>(u, h, g.ph_on[MU] && (s.x[MU] == 0), g, sg, A, X, Y);
   }
 }
 
-WL_D cplx<double> shfl_pair(cplx<double> v) {
+template <typename T>
+WL_D cplx<T> shfl_pair(cplx<T> v) {
   return {__shfl_xor_sync(0xffffffffu, v.re, 1), __shfl_xor_sync(0xffffffffu, v.im, 1)};
 }
 
-// Resident 256-thread blocks per SM: 2 caps the pair kernel at 128 registers
-// (no spills).  Measured at 24^3x48, 1 RHS: 96 us, against 148 us at 80
-// registers (3 blocks, spills) and 103 us for hop_kernel (144 registers).
+// Resident 256-thread blocks per SM the pair kernel is compiled for.  FP64: 2
+// caps it at 128 registers (no spills); measured at 24^3x48, 1 RHS: 96 us,
+// against 148 us at 80 registers (3 blocks, spills) and 103 us for hop_kernel
+// (144 registers).  FP32 storage and arithmetic: 3 (80 registers).
 #ifndef WL_HOP_PAIR_MINB
 #define WL_HOP_PAIR_MINB 2
 #endif
+#ifndef WL_HOP_PAIR_MINB_S
+#define WL_HOP_PAIR_MINB_S 3
+#endif
+template <class SF> struct PairMinBlocks {
+  static constexpr int value = WL_HOP_PAIR_MINB;
+};
+template <> struct PairMinBlocks<SpinorField<P_SINGLE>> {
+  static constexpr int value = WL_HOP_PAIR_MINB_S;
+};
 
-template <bool DAG, class LF, class EPI>
-__global__ void __launch_bounds__(256, WL_HOP_PAIR_MINB)
-    hop_pair_kernel(HopArgs<LF, SpinorField<P_DOUBLE>, EPI> A) {
+template <bool DAG, class LF, class SF, class EPI>
+__global__ void __launch_bounds__(256, PairMinBlocks<SF>::value) hop_pair_kernel(HopArgs<LF, SF, EPI> A) {
+  using T = typename SF::real;
+  static_assert(std::is_same<T, typename LF::real>::value, "links and spinors in the same arithmetic");
   const int c = blockIdx.x * (blockDim.x >> 1) + (threadIdx.x >> 1);
   const int j = threadIdx.x & 1;
-  const double sg = 1.0 - 2.0 * j;
+  const T sg = T(1) - T(2) * T(j);
   const int parity = A.parity0 ^ blockIdx.z;
   const int rhs = blockIdx.y;
   const bool act = c < A.g.Vh && rhs < A.nrhs && (A.mask == nullptr || A.mask[rhs] != 0);
-  cplx<double> Ac[3], Xc[3], Yc[3];
+  cplx<T> Ac[3], Xc[3], Yc[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) Ac[a] = Xc[a] = Yc[a] = {0.0, 0.0};
+  for (int a = 0; a < 3; ++a) Ac[a] = Xc[a] = Yc[a] = {T(0), T(0)};
   Site s{};
   if (act) {
     s = site_from_compact(A.g, parity, c);
-    const SpinorField<P_DOUBLE>& src = A.src[1 - parity];
+    const SF& src = A.src[1 - parity];
     pair_dir<0, DAG>(A.g, A.links, src, parity, s, rhs, j, sg, Ac, Xc, Yc);
     pair_dir<1, DAG>(A.g, A.links, src, parity, s, rhs, j, sg, Ac, Xc, Yc);
     pair_dir<2, DAG>(A.g, A.links, src, parity, s, rhs, j, sg, Ac, Xc, Yc);
     pair_dir<3, DAG>(A.g, A.links, src, parity, s, rhs, j, sg, Ac, Xc, Yc);
   }
   // thread 0 of the pair: a0 = A, a1 = A', a2 = Y + X', a3 = X + Y'
-  Spinor<double> acc;
+  Spinor<T> acc;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const cplx<double> Ap = shfl_pair(Ac[a]), Xp = shfl_pair(Xc[a]), Yp = shfl_pair(Yc[a]);
+    const cplx<T> Ap = shfl_pair(Ac[a]), Xp = shfl_pair(Xc[a]), Yp = shfl_pair(Yc[a]);
     acc.v[0][a] = Ac[a];
     acc.v[1][a] = Ap;
     acc.v[2][a] = Yc[a] + Xp;

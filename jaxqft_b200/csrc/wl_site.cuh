@@ -454,6 +454,21 @@ __global__ void cg_decide_kernel(CGScalars S, int n, int use_cond, cudaGraphCond
   }
 }
 
+// The WHILE node of a whole-solve graph (one iteration per body execution): continue while
+// any slot is active and fewer than `cap` iterations have run in this launch of the graph.
+struct SolveLoop {
+  const int* n_active;  // written by cg_finalize_kernel of the same iteration
+  int* count;           // zeroed before each launch of the graph
+  int cap;
+  cudaGraphConditionalHandle handle;
+};
+
+__global__ void solve_loop_kernel(SolveLoop L) {
+  const int c = *L.count + 1;
+  *L.count = c;
+  cudaGraphSetConditional(L.handle, (*L.n_active > 0 && c < L.cap) ? 1u : 0u);
+}
+
 __global__ void cg_finalize_kernel(CGScalars S, int n) {
   __shared__ int cnt;
   if (threadIdx.x == 0) cnt = 0;

@@ -125,6 +125,61 @@ def test_fp64_stencil_shapes(setup, forced, nslots):
     eng.close()
 
 
+# FP32 engines with fewer than four slots: thread-per-site and two-threads-per-site stencils
+FP32_CASES = [("1,64,1,0,1", 1), ("1,128,1,0,1", 3), ("1,256,1,0,1", 1), ("1,128,1,0", 1), ("2,64,2,0", 3)]
+
+
+@pytest.mark.parametrize("forced,nslots", FP32_CASES, indirect=["forced"])
+def test_fp32_stencil_shapes(setup, forced, nslots):
+    """Every FP32 iterated-stencil shape of a small engine (thread per site with 1 or 2 RHS,
+    two threads per site) gives the operator within the FP32
+    tolerance of the FP64 oracle, and its solves (FP64 reliable updates) reach an FP64 true
+    residual <= 1e-10 and are bitwise reproducible."""
+    shape, U, bc, ctx, gauge, rng = setup
+    m = -0.25
+    eng = Engine(ctx, gauge, nslots, op="eo_normal", inner="single")
+    xe = W.project(W.gaussian_spinor(rng, shape, 1), 0)
+    s = W.schur_even(U, xe, m, bc, normalized=True)
+    ref = W.schur_even(U, s, m, bc, normalized=True, dag=True)
+    out = eng.debug_apply(2, m, torch.from_numpy(xe[0])).cpu().numpy()
+    assert rel(out, ref[0]) < TOLS["single"], forced
+    eng.close()
+    eng = Engine(ctx, gauge, nslots, op="normal", inner="single")
+    x = W.gaussian_spinor(rng, shape, 1)
+    for stage, ref in ((4, W.apply_normal(U, x, m, bc)[0]), (3, W.apply_D(U, x, m, bc)[0])):
+        out = eng.debug_apply(stage, m, torch.from_numpy(x[0])).cpu().numpy()
+        assert rel(out, ref) < TOLS["single"], (forced, stage)
+    eng.close()
+    masses = np.linspace(-0.3, 0.1, nslots)
+    b = W.gaussian_spinor(rng, shape, nslots)
+    for op in ("eo_normal", "normal"):
+        bb = W.project(b, 0) if op == "eo_normal" else b
+        runs = []
+        for _ in range(2):
+            eng = Engine(ctx, gauge, nslots, op=op, inner="single", tol=1e-10, maxiter=3000)
+            eng.admit(np.arange(nslots), torch.from_numpy(bb), masses)
+            na = nslots
+            while na:
+                eng.step(8)
+                _, na = eng.poll()
+            xs = []
+            for r in range(nslots):
+                xr, st = eng.retire(r)
+                assert st["status"] == 2, (forced, op, r, st)
+                xs.append(xr.cpu().numpy())
+            eng.close()
+            runs.append(xs)
+        for r in range(nslots):
+            assert np.array_equal(runs[0][r], runs[1][r]), (forced, op, r)
+            xr = runs[0][r]
+            if op == "eo_normal":
+                s = W.schur_even(U, xr[None], masses[r], bc, normalized=True)
+                ax = W.schur_even(U, s, masses[r], bc, normalized=True, dag=True)[0]
+            else:
+                ax = W.apply_normal(U, xr[None], masses[r], bc)[0]
+            assert np.linalg.norm(bb[r] - ax) / np.linalg.norm(bb[r]) <= 1e-10, (forced, op, r)
+
+
 @pytest.fixture
 def forced_update(request):
     os.environ["WL_FORCE_UPDATE_TUNE"] = request.param
