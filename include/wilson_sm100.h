@@ -156,6 +156,12 @@ wl_status wl_engine_admit(wl_engine* eng, const int* slots, int n, const void* b
                           const double* tols, const int* maxiters);
 /* Run `iters` iterations on all active slots (asynchronous). */
 wl_status wl_engine_step(wl_engine* eng, int iters);
+/* Run up to `max_iters` iterations on all active slots in one launch, stopping
+   on the device as soon as a slot finishes (asynchronous; no counterpart in the
+   reference, whose solves are synchronous): a host loop driving many engines
+   then acts only when a slot can be retired.  Engines created without graphs
+   run `max_iters` iterations as wl_engine_step does. */
+wl_status wl_engine_run(wl_engine* eng, int max_iters);
 /* Synchronise and report per-slot status (0 idle, 1 running, 2..5 stopped). */
 wl_status wl_engine_poll(wl_engine* eng, int* status, int* n_active);
 /* Non-blocking form of wl_engine_poll, for a host loop that drives many

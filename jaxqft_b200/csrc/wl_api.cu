@@ -1165,6 +1165,13 @@ struct wl_engine {
   int loop_cap = 0;                // maxiter the loop graph was built for
   unsigned long long loop_gauge_id = 0;
   bool loop_failed = false;        // the loop graph could not be built: host-driven loop
+  // engine run (wl_engine_run): WHILE node that stops when a slot finishes or at a per-launch cap
+  cudaGraphExec_t grun = nullptr;
+  int* run_state = nullptr;        // device: [0] cap, [1] active count at launch start, [2] iterations
+  long long run_kernels = 0;       // unconditional kernels per run iteration
+  long long run_seen = 0;          // run iterations already counted into g_launches
+  unsigned long long run_gauge_id = 0;
+  bool run_failed = false;
   bool ru_links12 = false;         // FP64 true residual with 12-real links (links unitary to 1e-12)
 };
 
@@ -1854,6 +1861,7 @@ extern "C" void wl_engine_destroy(wl_engine* E) {
   if (st) cudaStreamSynchronize(st);
   if (E->gexec) cudaGraphExecDestroy(E->gexec);
   if (E->gloop) cudaGraphExecDestroy(E->gloop);
+  if (E->grun) cudaGraphExecDestroy(E->grun);
   IField* fs[] = {&E->b64, &E->x64, &E->y64, &E->t64, &E->xs, &E->rs, &E->p, &E->y, &E->t1};
   for (IField* f : fs) free_field(*f);
   cudaFree(E->dbl);
@@ -1862,6 +1870,7 @@ extern "C" void wl_engine_destroy(wl_engine* E) {
   cudaFree(E->counters);
   cudaFree(E->ru_iters);
   cudaFree(E->loop_count);
+  cudaFree(E->run_state);
   if (E->h_pinned) cudaFreeHost(E->h_pinned);
   if (E->poll_ev) cudaEventDestroy(E->poll_ev);
   if (st) cudaStreamDestroy(st);
@@ -1948,6 +1957,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   if (e == cudaSuccess) e = cudaMallocHost(&E->h_pinned, sizeof(int) * (3 * n + 2));
   if (e == cudaSuccess) e = cudaMalloc(&E->ru_iters, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&E->loop_count, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&E->run_state, 4 * sizeof(int));
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->poll_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     ctx->err = std::string("engine allocation: ") + cudaGetErrorString(e);
@@ -1958,6 +1968,7 @@ extern "C" wl_status wl_engine_create(wl_ctx* ctx, wl_gauge* G, const wl_solve_p
   cudaMemsetAsync(E->ints, 0, sizeof(int) * (kEngineInts * n + 1), st);
   cudaMemsetAsync(E->counters, 0, sizeof(unsigned) * (n + 1), st);
   cudaMemsetAsync(E->ru_iters, 0, sizeof(int), st);
+  cudaMemsetAsync(E->run_state, 0, 4 * sizeof(int), st);
   double* d = E->dbl;
   E->r2 = d + 0 * n; E->r2_new = d + 1 * n; E->pAp = d + 2 * n; E->r2_true = d + 3 * n;
   E->rmax2 = d + 4 * n; E->b2 = d + 5 * n; E->tol2 = d + 6 * n; E->beta = d + 7 * n;
@@ -2140,7 +2151,7 @@ static wl_status build_graph(wl_engine* E, cudaStream_t st) {
 // long before).  wl_solve launches it once per solve instead of launching an iteration graph
 // and synchronising on a status poll every check_every iterations.  On any failure the
 // engine keeps the host-driven loop.
-static wl_status build_loop_graph(wl_engine* E, cudaStream_t st) {
+static wl_status build_loop_graph(wl_engine* E, cudaStream_t st, bool run_mode = false) {
   wl_ctx* ctx = E->ctx;
   cudaGraph_t graph = nullptr;
   WL_CUDA(ctx, cudaGraphCreate(&graph, 0));
@@ -2163,21 +2174,54 @@ static wl_status build_loop_graph(wl_engine* E, cudaStream_t st) {
   if (e == cudaSuccess) {
     int cap = 0;
     for (int m : E->h_maxiter) cap = std::max(cap, m);
-    SolveLoop L{E->n_active, E->loop_count, cap + 8, wh};
+    SolveLoop L{E->n_active, E->loop_count, cap + 8, wh, nullptr, nullptr, nullptr};
+    if (run_mode) L = SolveLoop{E->n_active, E->run_state + 2, 0, wh, E->run_state, E->run_state + 1, E->run_state + 3};
     e = capture_iteration(E, st, body, &L, &nk);
   }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&E->gloop, graph, 0);
+  cudaGraphExec_t& exec = run_mode ? E->grun : E->gloop;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) {
-    E->gloop = nullptr;
-    E->loop_failed = true;
+    exec = nullptr;
+    (run_mode ? E->run_failed : E->loop_failed) = true;
     cudaGetLastError();
     return WL_ERR_CUDA;
+  }
+  if (run_mode) {
+    E->run_kernels = nk;
+    return WL_OK;
   }
   E->loop_kernels = nk;
   E->loop_cap = 0;
   for (int m : E->h_maxiter) E->loop_cap = std::max(E->loop_cap, m);
   return WL_OK;
+}
+
+// Up to max_iters iterations in one launch of the engine's run graph, stopping on the device
+// as soon as a slot finishes (see solve_loop_kernel); engines without graphs step instead.
+extern "C" wl_status wl_engine_run(wl_engine* E, int max_iters) {
+  NvtxRange nvtx_range("wl_engine_run");
+  if (!E) WL_FAIL(nullptr, WL_ERR_ARG, "null engine");
+  if (max_iters <= 0) WL_FAIL(E->ctx, WL_ERR_ARG, "max_iters must be positive");
+  wl_ctx* ctx = E->ctx;
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (!E->prm.use_graph || E->run_failed) return wl_engine_step(E, max_iters);
+  cudaStream_t st = engine_stream(E);
+  if (E->grun && E->run_gauge_id != E->gauge->id) {
+    cudaGraphExecDestroy(E->grun);
+    E->grun = nullptr;
+  }
+  if (!E->grun) {
+    if (build_loop_graph(E, st, true) != WL_OK) {
+      ctx->err.clear();
+      return wl_engine_step(E, max_iters);
+    }
+    E->run_gauge_id = E->gauge->id;
+  }
+  g_launches++;
+  run_loop_setup_kernel<<<1, 1, 0, st>>>(E->run_state, max_iters, E->run_state + 1, E->n_active, E->run_state + 2);
+  WL_CUDA(ctx, cudaGraphLaunch(E->grun, st));
+  return check_launch(ctx, "wl_engine_run");
 }
 
 extern "C" wl_status wl_engine_step(wl_engine* E, int iters) {
@@ -2283,6 +2327,7 @@ static wl_status enqueue_poll_copies(wl_engine* E, cudaStream_t st) {
   WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned, E->n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
   WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned + 1, E->status, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
   WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned + 1 + n, E->ru_iters, sizeof(int), cudaMemcpyDeviceToHost, st));
+  WL_CUDA(ctx, cudaMemcpyAsync(E->h_pinned + 3 + n, E->run_state + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
   return WL_OK;
 }
 
@@ -2293,6 +2338,9 @@ static void read_poll_copies(wl_engine* E, int* status, int* n_active) {
     const long long seen = E->h_pinned[1 + n];
     g_launches += (seen - E->ru_iters_seen) * E->ru_body_kernels;
     E->ru_iters_seen = seen;
+    const long long runs = E->h_pinned[3 + n];  // iterations run by wl_engine_run launches
+    g_launches += (runs - E->run_seen) * E->run_kernels;
+    E->run_seen = runs;
   }
   if (n_active) *n_active = E->h_pinned[0];
   if (status) std::memcpy(status, E->h_pinned + 1, sizeof(int) * n);

@@ -454,19 +454,37 @@ __global__ void cg_decide_kernel(CGScalars S, int n, int use_cond, cudaGraphCond
   }
 }
 
-// The WHILE node of a whole-solve graph (one iteration per body execution): continue while
-// any slot is active and fewer than `cap` iterations have run in this launch of the graph.
+// The WHILE node of a device-side iteration loop (one iteration per body execution).
+// Whole solve (wl_solve): continue while any slot is active and fewer than `cap`
+// iterations have run in this launch.  Engine run (wl_engine_run): the cap is read from
+// `capd` (set per launch), and the loop also stops as soon as a slot has finished, i.e.
+// the active count fell below its value at the start of the launch (`start`), so the
+// host can retire it.
 struct SolveLoop {
   const int* n_active;  // written by cg_finalize_kernel of the same iteration
-  int* count;           // zeroed before each launch of the graph
+  int* count;           // iterations of this launch (zeroed before each launch)
   int cap;
   cudaGraphConditionalHandle handle;
+  const int* capd;      // engine run: per-launch cap (else nullptr: cap)
+  const int* start;     // engine run: active count at the start of the launch (else nullptr)
+  int* total;           // engine run: iterations over all launches (else nullptr)
 };
 
 __global__ void solve_loop_kernel(SolveLoop L) {
   const int c = *L.count + 1;
   *L.count = c;
-  cudaGraphSetConditional(L.handle, (*L.n_active > 0 && c < L.cap) ? 1u : 0u);
+  if (L.total) *L.total += 1;
+  const int na = *L.n_active;
+  const int cap = L.capd ? *L.capd : L.cap;
+  const bool more = na > 0 && c < cap && (L.start == nullptr || na >= *L.start);
+  cudaGraphSetConditional(L.handle, more ? 1u : 0u);
+}
+
+// Per-launch state of an engine run: the cap, the active count at the start, the count reset.
+__global__ void run_loop_setup_kernel(int* capd, int cap, int* start, const int* n_active, int* count) {
+  *capd = cap;
+  *start = *n_active;
+  *count = 0;
 }
 
 __global__ void cg_finalize_kernel(CGScalars S, int n) {

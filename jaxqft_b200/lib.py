@@ -39,7 +39,7 @@ EXPORTS = (
     "wl_version", "wl_ctx_create", "wl_ctx_destroy", "wl_last_error", "wl_ctx_set_stream",
     "wl_ctx_synchronize", "wl_eo_maps", "wl_gauge_create", "wl_gauge_update", "wl_gauge_unitarity",
     "wl_gauge_destroy", "wl_apply", "wl_solve", "wl_engine_create", "wl_engine_destroy", "wl_engine_admit",
-    "wl_engine_step", "wl_engine_poll", "wl_engine_poll_async", "wl_engine_poll_ready", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
+    "wl_engine_step", "wl_engine_run", "wl_engine_poll", "wl_engine_poll_async", "wl_engine_poll_ready", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
     "wl_engine_stream", "wl_engine_time_hop", "wl_engine_time_update_hop", "wl_kernel_launches", "wl_engine_debug_apply",
     "wl_apply_schur_normal_noalloc", "wl_gauge_force", "wl_gauge_evolve", "wl_gauge_plaquette_sum",
     "wl_momentum_kinetic", "wl_pion_correlator", "wl_bounds_errors", "wl_random_spinor", "wl_random_algebra",
@@ -101,6 +101,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wl_engine_destroy": (None, [vp]),
         "wl_engine_admit": (i, [vp, pi, i, vp, pd, pd, pi]),
         "wl_engine_step": (i, [vp, i]),
+        "wl_engine_run": (i, [vp, i]),
         "wl_engine_poll": (i, [vp, pi, pi]),
         "wl_engine_poll_async": (i, [vp]),
         "wl_engine_poll_ready": (i, [vp, pi, pi]),
@@ -475,6 +476,11 @@ class Engine:
 
     def step(self, iters: int):
         self.ctx._check(self.ctx.lib.wl_engine_step(self.handle, int(iters)))
+
+    def run(self, max_iters: int):
+        """Up to max_iters iterations in one graph launch; stops on the device as soon as a
+        slot finishes (asynchronous, like step)."""
+        self.ctx._check(self.ctx.lib.wl_engine_run(self.handle, int(max_iters)))
 
     def poll(self):
         st = np.zeros(self.nslots, dtype=np.int32)

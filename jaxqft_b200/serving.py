@@ -115,12 +115,16 @@ class PropagatorServer:
     def __init__(self, volumes: Sequence[Tuple[int, ...]], gauge_seeds: Sequence[int] = (0, 1, 2, 3),
                  link_scale: float = 0.2, nslots: int = 16, inner: str = "half", tol: float = 1e-10,
                  maxiter: int = 4000, hbm_budget_bytes: Optional[int] = None, iters_per_poll: int = 8,
-                 device=None, keep_solutions: bool = True):
+                 run_cap: int = 256, device_runs: bool = True, device=None, keep_solutions: bool = True):
         if not torch.cuda.is_available():
             raise RuntimeError("the serving loop requires a CUDA device")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.nslots, self.inner, self.tol, self.maxiter = int(nslots), inner, float(tol), int(maxiter)
         self.iters_per_poll = int(iters_per_poll)
+        self.run_cap = int(run_cap)
+        # False: drive the engines with iters_per_poll iterations per poll (wl_engine_step), as
+        # before device-side runs, for comparisons
+        self.device_runs = bool(device_runs)
         # False: a finished request's device buffers (sources, right-hand sides, solutions) are
         # released as soon as it completes, as a server does once the response has been sent;
         # only its statistics (and its pion correlator) are kept
@@ -213,11 +217,15 @@ class PropagatorServer:
         """Serve `requests` (arrival times in seconds from the start).
 
         The host never waits on one engine while another could work: every busy
-        engine with nothing queued gets `iters_per_poll` CG iterations and a
-        non-blocking status poll on its own stream (wl_engine_poll_async); the loop
-        then admits arrivals, and handles each engine whose poll has landed
-        (wl_engine_poll_ready) by retiring its converged slots and queueing its next
-        iterations.  `self.trace` samples (seconds, queued requests, busy slots)."""
+        engine with nothing in flight gets one device-side run of CG iterations
+        (wl_engine_run: it stops by itself as soon as one of its slots finishes) and
+        a non-blocking status poll on its own stream (wl_engine_poll_async); the
+        loop then admits arrivals, and handles each engine whose poll has landed
+        (wl_engine_poll_ready) by retiring its converged slots and starting its next
+        run.  A run is capped at about the time of `iters_per_poll` iterations on the
+        largest served volume (`run_iters`), because a request admitted into an
+        engine starts iterating only when the engine's current run ends.
+        `self.trace` samples (seconds, queued requests, busy slots)."""
         pending = collections.deque(sorted(requests, key=lambda r: r.t_arrive))
         t0 = time_fn()
         inflight = set()
@@ -231,7 +239,10 @@ class PropagatorServer:
                 self._try_admit(now)
             for key, e in self.engines.items():
                 if e.owner and key not in inflight:
-                    e.engine.step(self.iters_per_poll)
+                    if self.device_runs:
+                        e.engine.run(self.run_iters(key[0]))
+                    else:
+                        e.engine.step(self.iters_per_poll)
                     e.engine.poll_async()
                     inflight.add(key)
             landed = False
@@ -267,6 +278,14 @@ class PropagatorServer:
         if self.device.type == "cuda":
             torch.cuda.synchronize(self.device)
         return self.done
+
+    def run_iters(self, volume) -> int:
+        """Iteration cap of one device-side run on `volume`: iters_per_poll scaled by the
+        largest served volume over this one (an iteration's time grows with the volume),
+        between iters_per_poll and run_cap."""
+        vmax = max(int(np.prod(v)) for v in self.ctx)
+        scaled = self.iters_per_poll * vmax // max(1, int(np.prod(volume)))
+        return int(max(self.iters_per_poll, min(self.run_cap, scaled)))
 
     def _measure_pion(self, req: Request) -> None:
         if req.kind != "point" or req.nrhs != 12:
@@ -372,12 +391,19 @@ def main(argv=None):
     ap.add_argument("--rates", default="50", help="comma-separated mean arrival rates (requests/s)")
     ap.add_argument("--seconds", type=float, default=30.0, help="arrival window per rate")
     ap.add_argument("--inner", default="half")
+    ap.add_argument("--compare-runs", action="store_true",
+                    help="serve each rate twice per seed, with device-side runs and host-stepped engines")
+    ap.add_argument("--seeds", default="1", help="comma-separated request-stream seeds")
     args = ap.parse_args(argv)
     server = PropagatorServer(VOLUMES, gauge_seeds=(0, 1, 2, 3), nslots=16, inner=args.inner, keep_solutions=False)
     warm_server(server)
-    for rate in (float(r) for r in args.rates.split(",")):
-        s = serve_once(server, rate, args.seconds)
-        print(json.dumps({"serve": True, **s}), flush=True)
+    modes = (True, False) if args.compare_runs else (True,)
+    for seed in (int(x) for x in args.seeds.split(",")):
+        for rate in (float(r) for r in args.rates.split(",")):
+            for mode in modes:
+                server.device_runs = mode
+                s = serve_once(server, rate, args.seconds, seed=seed)
+                print(json.dumps({"serve": True, "device_runs": mode, "seed": seed, **s}), flush=True)
     server.close()
 
 

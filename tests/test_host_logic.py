@@ -64,7 +64,8 @@ class FakeCtx:
 
 
 class FakeEngine:
-    """Slots converge `solve_steps` step() calls after their admission."""
+    """Slots converge `solve_steps` iterations (step() calls of one iteration) after their
+    admission; run() iterates until a slot finishes."""
 
     solve_steps = 3
     created = []
@@ -86,6 +87,16 @@ class FakeEngine:
     def step(self, n):
         for s in self.left:
             self.left[s] = max(0, self.left[s] - 1)
+
+    def run(self, n):
+        # as wl_engine_run: steps until a running slot finishes, at most n
+        for _ in range(n):
+            running = [s for s, k in self.left.items() if k > 0]
+            if not running:
+                break
+            self.step(1)
+            if any(self.left[s] == 0 for s in running):
+                break
 
     def poll(self):
         st = np.zeros(self.nslots, dtype=np.int32)
@@ -113,6 +124,7 @@ def make_server(volumes, nslots, budget, engine_bytes):
     srv = object.__new__(serving.PropagatorServer)
     srv.device = torch.device("cpu")
     srv.nslots, srv.inner, srv.tol, srv.maxiter, srv.iters_per_poll = nslots, "half", 1e-10, 100, 8
+    srv.run_cap, srv.device_runs = 256, True
     srv.keep_solutions = True
     srv.hbm_budget = budget
     srv.ctx = {v: FakeCtx(v, engine_bytes) for v in volumes}
