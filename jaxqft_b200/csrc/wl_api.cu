@@ -255,12 +255,15 @@ static bool half_color_enabled() {
   return on;
 }
 
-// WL_HALF_ACC=1: the 16-lane FP16 hop also accumulates its eight contributions in packed FP16
-// (relative weights, lane_site_hh), for comparisons.
+// The 16-lane FP16 hop accumulates its eight contributions in packed FP16 (relative weights,
+// lane_site_hh) and is compiled for 8 resident blocks per SM; WL_HALF_ACC=0 selects FP32
+// accumulation (per-epilogue register caps) for comparisons.  Measured at 24^3x48 with 16 RHS,
+// two interleaved rounds on one box: 49.9-50.1 solves/s against 48.8-49.0 (hop 0.281-0.297 ms
+// against 0.296-0.315), 157-165 CG iterations against 156-165, every true residual <= 1e-10.
 static bool half_acc_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("WL_HALF_ACC");
-    return e && e[0] == '1';
+    return !(e && e[0] == '0');
   }();
   return on;
 }

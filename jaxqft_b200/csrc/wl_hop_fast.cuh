@@ -260,6 +260,12 @@ constexpr int kLaneBlock = 128;
 #ifndef WL_LANE_MIN_BLOCKS_XPAY
 #define WL_LANE_MIN_BLOCKS_XPAY WL_LANE_MIN_BLOCKS
 #endif
+// The FP16-accumulation form (HA) holds its sums as half2 and needs fewer registers: 8 blocks
+// (64 registers) for every epilogue measured faster than the split above (49.9-50.1 against
+// 49.3-49.5 solves/s in interleaved whole-solve runs at 24^3x48 with 16 RHS).
+#ifndef WL_LANE_MIN_BLOCKS_HA
+#define WL_LANE_MIN_BLOCKS_HA 8
+#endif
 template <class SF>
 struct EpiCG;  // wl_site.cuh
 template <bool DAG, class EPI>
@@ -703,7 +709,8 @@ WL_D void reduce_lanes(double v, const Reduce& Rd, int nrhs, const int* /*mask*/
 }
 
 template <bool DAG, int R, class LF, class SF, class EPI, bool HC = false, bool HA = false>
-__global__ void __launch_bounds__(kLaneBlock, LaneMinBlocks<DAG, EPI>::value) hop_lanes_kernel(HopArgs<LF, SF, EPI> A) {
+__global__ void __launch_bounds__(kLaneBlock, HA ? WL_LANE_MIN_BLOCKS_HA : LaneMinBlocks<DAG, EPI>::value)
+    hop_lanes_kernel(HopArgs<LF, SF, EPI> A) {
   static_assert(!HC || std::is_same<SF, SpinorField<P_HALF>>::value, "FP16 colour multiply needs FP16 fields");
   static_assert(!HA || HC, "FP16 accumulation runs behind the FP16 colour multiply");
   constexpr int S = kLaneBlock / R;

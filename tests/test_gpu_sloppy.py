@@ -179,3 +179,42 @@ def test_fp16_hop_with_fp32_colour_multiply():
     res = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True,
                          timeout=600)
     assert res.returncode == 0 and "fp32 colour ok" in res.stdout, res.stdout[-2000:] + res.stderr[-4000:]
+
+
+def test_fp16_lanes_hop_with_fp32_accumulation():
+    """The 16-lane FP16 hop sums its eight contributions in packed FP16 by default; the FP32
+    accumulation form (WL_HALF_ACC=0, kept for comparisons; read once per process) must meet
+    the same FP16 operator bound and solve 16 RHS to an FP64 true residual <= 1e-10, checked
+    in a child process."""
+    import os
+    import subprocess
+    import sys
+
+    from tests.conftest import ROOT
+
+    code = ("import os, tests.test_gpu_sloppy as T, numpy as np, torch\n"
+            "from oracle import wilson as W\n"
+            "shape = (4, 4, 4, 8); bc = (1, 1, 1, -1); rng = np.random.default_rng(8)\n"
+            "U = W.hot_links(rng, shape, 1, 0.2)\n"
+            "ctx = T.WilsonContext(shape, bc=bc); g = ctx.gauge(torch.from_numpy(U[0]))\n"
+            "m = -0.2962963; os.environ['WL_FORCE_TUNE'] = '1,128,1,16'\n"
+            "eng = T.Engine(ctx, g, 16, op='eo_normal', inner='half', tol=1e-10, maxiter=3000)\n"
+            "for src, x in T._fields(shape, 1).items():\n"
+            "    xe = W.project(x[None], 0)\n"
+            "    ref = W.schur_even(U, W.schur_even(U, xe, m, bc, normalized=True), m, bc, normalized=True, dag=True)\n"
+            "    out = eng.debug_apply(2, m, torch.from_numpy(xe[0])).cpu().numpy()\n"
+            "    assert T.rel(out, ref[0]) < T.TOLS['half'], (src, T.rel(out, ref[0]))\n"
+            "b = W.project(W.gaussian_spinor(rng, shape, 16), 0)\n"
+            "eng.admit(np.arange(16), torch.from_numpy(b), np.full(16, m))\n"
+            "na = 16\n"
+            "while na:\n"
+            "    eng.step(8); _, na = eng.poll()\n"
+            "for r in range(16):\n"
+            "    xr, st = eng.retire(r); xr = xr.cpu().numpy()[None]\n"
+            "    ax = W.schur_even(U, W.schur_even(U, xr, m, bc, normalized=True), m, bc, normalized=True, dag=True)[0]\n"
+            "    assert st['status'] == 2 and np.linalg.norm(b[r] - ax) / np.linalg.norm(b[r]) <= 1e-10, (r, st)\n"
+            "print('fp32 accumulation ok')\n")
+    env = dict(os.environ, WL_HALF_ACC="0")
+    res = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True,
+                         timeout=600)
+    assert res.returncode == 0 and "fp32 accumulation ok" in res.stdout, res.stdout[-2000:] + res.stderr[-4000:]
