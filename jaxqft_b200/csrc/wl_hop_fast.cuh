@@ -262,7 +262,8 @@ constexpr int kLaneBlock = 128;
 #endif
 // The FP16-accumulation form (HA) holds its sums as half2 and needs fewer registers: 8 blocks
 // (64 registers) for every epilogue measured faster than the split above (49.9-50.1 against
-// 49.3-49.5 solves/s in interleaved whole-solve runs at 24^3x48 with 16 RHS).
+// 49.3-49.5 solves/s in interleaved whole-solve runs at 24^3x48 with 16 RHS) and than 9 blocks
+// (56 registers, 20-byte spills: 48.7-48.9 against 49.1-49.5).
 #ifndef WL_LANE_MIN_BLOCKS_HA
 #define WL_LANE_MIN_BLOCKS_HA 8
 #endif
