@@ -15,7 +15,8 @@ Reported: value = solves/s of that batched mixed solve (device time, CUDA
 events on the solver stream, inputs resident in HBM), next to plain FP64 CG
 (one RHS at a time) on the same systems; e2e = the same solve through the
 public API from pinned host buffers with host<->device copies timed; the
-roofline of the dominant kernel (the FP16 16-RHS hop) measured live; the
+roofline of the dominant kernel (the fused CG hop, the FP16 16-RHS stencil with
+the CG update in its epilogue; the plain stencil beside it) measured live; the
 Dslash bandwidth (FP64, 1 RHS) in the internal layout and in the reference
 layout; and a CPU baseline (the C restatement of the reference's CG on the
 host cores).
@@ -279,11 +280,19 @@ def run_ours(args):
                                     "flops_per_site_dslash x Vh"))
     eng64.close()
 
-    # ---- live roofline of the dominant kernel (FP16 hop over 16 RHS)
+    # ---- live rooflines of the FP16 16-RHS hops: the plain stencil (K_oe p) and, below, the dominant kernel
     hop_ms, hop_bytes = eng.time_hop(reps=20)
     hbm, peak_kind = peaks()
     achieved = hop_bytes / (hop_ms * 1e-3) / 1e9
     traffic = profile_traffic(f"hop_h12_half_nrhs{NRHS}_{'x'.join(map(str, SHAPE))}")
+    # The dominant kernel of the timed solve is the fused CG hop (the fourth hop of an iteration,
+    # with x_s += alpha p, r_s -= alpha A p and |r_s|^2 in its epilogue): the largest share of the
+    # ncu launch list of a CG iteration.  Timed the same way; it rewrites the slots' x_s and r_s,
+    # and this engine solves nothing after it.
+    eng.time_hop(reps=3, cg=True)
+    cg_ms, cg_bytes = eng.time_hop(reps=20, cg=True)
+    cg_achieved = cg_bytes / (cg_ms * 1e-3) / 1e9
+    cg_traffic = profile_traffic(f"hop_cg_h12_half_nrhs{NRHS}_{'x'.join(map(str, SHAPE))}")
 
     # ---- the drop-in FP64 Dslash (reference layout, apply_D), 1 RHS: GB/s against the same peak
     psi1 = eta[NRHS - 1:NRHS].contiguous()
@@ -395,13 +404,24 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, SHAPE)), "kappa": KAPPA,
                        "nrhs": NRHS, "tol": TOL, "parallelism": f"replicas x{world} (independent solves)",
                        "l2": "working set > 126 MB L2 (no flush needed)"},
-            "roofline": {"bound": "hbm", "kernel": "hop (FP16 storage, 12-real links, 16 RHS, EO parity)",
-                         "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": hop_bytes,
-                         "ms_per_launch": hop_ms, "traffic": traffic,
-                         **naive_rate(np.prod(SHAPE) // 2, NRHS, 52, 24, hop_ms),
-                         **ref_gflops(DIRAC.flops_per_site_dslash(3) * int(np.prod(SHAPE)) // 2 * NRHS, hop_ms,
-                                      "flops_per_site_dslash x Vh x 16 RHS")},
+            "roofline": {"bound": "hbm",
+                         "kernel": "fused CG hop: M^dag y with x_s += alpha p, r_s -= alpha Ap, |r_s|^2 (FP16 storage, "
+                                   "12-real links, 16 RHS, EO parity); the largest share of a CG iteration",
+                         "achieved": cg_achieved, "peak": hbm, "unit": "GB/s", "frac": cg_achieved / hbm,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": cg_bytes,
+                         "bytes_per_site": "8 links x 24 B + 16 RHS x 7 records x 52 B (gathered source; y, p, "
+                                           "x_s, r_s read; x_s, r_s written)",
+                         "ms_per_launch": cg_ms, "traffic": cg_traffic,
+                         **ref_gflops(DIRAC.flops_per_site_dslash(3) * int(np.prod(SHAPE)) // 2 * NRHS, cg_ms,
+                                      "flops_per_site_dslash x Vh x 16 RHS (stencil only)")},
+            "roofline_plain_hop": {"bound": "hbm", "kernel": "hop K_oe p (FP16 storage, 12-real links, 16 RHS, "
+                                                             "EO parity), no epilogue fields",
+                                   "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                                   "peak_kind": peak_kind, "algorithmic_bytes_per_launch": hop_bytes,
+                                   "ms_per_launch": hop_ms, "traffic": traffic,
+                                   **naive_rate(np.prod(SHAPE) // 2, NRHS, 52, 24, hop_ms),
+                                   **ref_gflops(DIRAC.flops_per_site_dslash(3) * int(np.prod(SHAPE)) // 2 * NRHS,
+                                                hop_ms, "flops_per_site_dslash x Vh x 16 RHS")},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,

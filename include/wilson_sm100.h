@@ -188,6 +188,12 @@ wl_status wl_engine_time_hop(wl_engine* eng, int reps, double* ms_per_launch, do
 /* The same for the FP64 hop of the reliable update (x64 -> K_oe x64 over all
    slots, with the FP64 links and the shape the update uses). */
 wl_status wl_engine_time_update_hop(wl_engine* eng, int reps, double* ms_per_launch, double* bytes_per_launch);
+/* The same for the fused CG hop, the fourth hop of an iteration with the CG
+   update in its epilogue (x_s += alpha p, r_s -= alpha A p, |r_s|^2); bytes =
+   8 links per target site plus, per RHS, the gathered source and the y, p, x_s,
+   r_s records read and x_s, r_s written.  It changes the slots' iteration
+   fields: admit the slots again before stepping them. */
+wl_status wl_engine_time_cg_hop(wl_engine* eng, int reps, double* ms_per_launch, double* bytes_per_launch);
 /* Apply the engine's iterated (sloppy-precision) operator to one
    reference-layout field through slot 0's buffers, for testing the FP16/FP32
    operators against FP64: stage 0 -> K_oe x_e (odd sites of out), 1 -> M x_e,

@@ -1342,6 +1342,47 @@ static void time_hop_impl(wl_engine* E, cudaStream_t st, int reps, float* ms) {
   cudaEventDestroy(e1);
 }
 
+// The fused CG hop, timed like time_hop_impl: the fourth hop of an iteration (M^dag y for the
+// EO operator, D^dag y for the full one) with the CG update in its epilogue (x_s += alpha p,
+// r_s -= alpha A p, |r_s|^2 partials) over all slots, the kernel alone (no finalize).  It
+// updates x_s and r_s in place, so the slots must be admitted again before they iterate.
+template <int S>
+static void time_cg_hop_impl(wl_engine* E, cudaStream_t st, int reps, float* ms) {
+  using SFS = SpinorField<S>;
+  using LS = typename SloppyLinks<S>::type;
+  const bool eo = E->prm.op == WL_SOLVE_EO_NORMAL;
+  HopArgs<LS, SFS, EpiCG<SFS>> A{};
+  A.g = E->ctx->g;
+  A.links = SloppyLinks<S>::get(E->gauge);
+  sf2<S>(eo ? E->t1 : E->y, A.src);
+  A.parity0 = 0;
+  A.nrhs = E->n;
+  A.mask = nullptr;
+  sf2<S>(E->y, A.epi.y);
+  sf2<S>(E->p, A.epi.p);
+  sf2<S>(E->xs, A.epi.xs);
+  sf2<S>(E->rs, A.epi.rs);
+  A.epi.a = eo ? E->one : E->m0;
+  A.epi.b = eo ? E->half_alpha : E->neg_half;
+  A.epi.r2 = E->r2;
+  A.epi.pAp = E->pAp;
+  A.epi.alpha = E->alpha;
+  A.red = red_to(E, E->r2_new);
+  const int npar = eo ? 1 : 2;
+  const Tune t = effective_tune<IdxCompact, SFS, EpiCG<SFS>>(E->ts);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  launch_hop_impl<true, IdxCompact>(t, A, npar, st);
+  cudaEventRecord(e0, st);
+  for (int i = 0; i < reps; ++i) launch_hop_impl<true, IdxCompact>(t, A, npar, st);
+  cudaEventRecord(e1, st);
+  cudaEventSynchronize(e1);
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+}
+
 // Enqueue the FP64 normal operator on x64 ending in the true residual
 // rs = convert(b - A x64), r2_true = |b - A x64|^2, for the slots in `mask`.
 template <int S, class LDT>
@@ -2271,6 +2312,29 @@ extern "C" wl_status wl_engine_time_hop(wl_engine* E, int reps, double* ms, doub
   if (s != WL_OK) return s;
   *ms = (double)t / reps;
   *bytes = (double)hop_bytes(ctx->g, E->sprec, E->n);
+  return WL_OK;
+}
+
+extern "C" wl_status wl_engine_time_cg_hop(wl_engine* E, int reps, double* ms, double* bytes) {
+  if (!E || !ms || !bytes || reps <= 0) WL_FAIL(nullptr, WL_ERR_ARG, "bad argument");
+  wl_ctx* ctx = E->ctx;
+  WL_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = engine_stream(E);
+  float t = 0.f;
+  switch (E->sprec) {
+    case P_HALF: time_cg_hop_impl<P_HALF>(E, st, reps, &t); break;
+    case P_SINGLE: time_cg_hop_impl<P_SINGLE>(E, st, reps, &t); break;
+    default: time_cg_hop_impl<P_DOUBLE>(E, st, reps, &t); break;
+  }
+  wl_status s = check_launch(ctx, "wl_engine_time_cg_hop");
+  if (s != WL_OK) return s;
+  *ms = (double)t / reps;
+  // per target site: 8 links; per RHS the source record gathered once, the self records of
+  // y, p, x_s and r_s read and x_s, r_s written
+  const double L = E->sprec == P_DOUBLE ? 144.0 : (E->sprec == P_SINGLE ? 48.0 : 24.0);
+  const double S = E->sprec == P_DOUBLE ? 192.0 : (E->sprec == P_SINGLE ? 96.0 : 52.0);
+  const double sites = (double)ctx->g.Vh * (E->prm.op == WL_SOLVE_EO_NORMAL ? 1 : 2);
+  *bytes = sites * (8.0 * L + E->n * 7.0 * S);
   return WL_OK;
 }
 

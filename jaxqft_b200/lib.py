@@ -40,7 +40,7 @@ EXPORTS = (
     "wl_ctx_synchronize", "wl_eo_maps", "wl_gauge_create", "wl_gauge_update", "wl_gauge_unitarity",
     "wl_gauge_destroy", "wl_apply", "wl_solve", "wl_engine_create", "wl_engine_destroy", "wl_engine_admit",
     "wl_engine_step", "wl_engine_run", "wl_engine_poll", "wl_engine_poll_async", "wl_engine_poll_ready", "wl_engine_retire", "wl_engine_bytes", "wl_pf_force",
-    "wl_engine_stream", "wl_engine_time_hop", "wl_engine_time_update_hop", "wl_kernel_launches", "wl_engine_debug_apply",
+    "wl_engine_stream", "wl_engine_time_hop", "wl_engine_time_update_hop", "wl_engine_time_cg_hop", "wl_kernel_launches", "wl_engine_debug_apply",
     "wl_apply_schur_normal_noalloc", "wl_gauge_force", "wl_gauge_evolve", "wl_gauge_plaquette_sum",
     "wl_momentum_kinetic", "wl_pion_correlator", "wl_bounds_errors", "wl_random_spinor", "wl_random_algebra",
     "wl_field_dots", "wl_field_combine",
@@ -111,6 +111,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wl_engine_stream": (vp, [vp]),
         "wl_engine_time_hop": (i, [vp, i, pd, pd]),
         "wl_engine_time_update_hop": (i, [vp, i, pd, pd]),
+        "wl_engine_time_cg_hop": (i, [vp, i, pd, pd]),
         "wl_kernel_launches": (ctypes.c_int64, []),
         "wl_bounds_errors": (ctypes.c_int64, [ctypes.POINTER(ctypes.c_longlong)]),
         "wl_engine_debug_apply": (i, [vp, i, d, vp, vp]),
@@ -535,11 +536,13 @@ class Engine:
         self.ctx._check(self.ctx.lib.wl_engine_debug_apply(self.handle, int(stage), float(mass), _ptr(x), _ptr(out)))
         return out
 
-    def time_hop(self, reps: int = 20, update: bool = False):
-        """(ms per launch, algorithmic bytes per launch) of the iterated hop kernel, or with
-        update=True of the FP64 hop of the reliable update."""
+    def time_hop(self, reps: int = 20, update: bool = False, cg: bool = False):
+        """(ms per launch, algorithmic bytes per launch) of the iterated hop kernel, with
+        update=True of the FP64 hop of the reliable update, with cg=True of the fused CG hop
+        (which changes the slots' fields: admit them again before stepping)."""
         ms, by = ctypes.c_double(), ctypes.c_double()
-        fn = self.ctx.lib.wl_engine_time_update_hop if update else self.ctx.lib.wl_engine_time_hop
+        fn = (self.ctx.lib.wl_engine_time_update_hop if update else
+              self.ctx.lib.wl_engine_time_cg_hop if cg else self.ctx.lib.wl_engine_time_hop)
         self.ctx._check(fn(self.handle, int(reps), ctypes.byref(ms), ctypes.byref(by)))
         return float(ms.value), float(by.value)
 
