@@ -90,6 +90,7 @@ class FakeEngine:
 
     def run(self, n):
         # as wl_engine_run: steps until a running slot finishes, at most n
+        self.run_caps = getattr(self, "run_caps", []) + [n]
         for _ in range(n):
             running = [s for s, k in self.left.items() if k > 0]
             if not running:
@@ -229,3 +230,28 @@ def test_poisson_requests_statistics():
     n = np.array([r.nrhs for r in reqs])
     assert k.min() >= 0.120 and k.max() <= 0.135 and n.min() == 1 and n.max() == 12
     assert math.isclose(np.mean([r.kind == "point" for r in reqs]), 0.5, abs_tol=0.05)
+
+
+def test_serving_run_caps_scale_with_volume(fake_engines):
+    """Device-side runs are capped at iters_per_poll on the largest served volume and at
+    proportionally more iterations on smaller ones (a similar wall time per run), within
+    [iters_per_poll, run_cap]; host-stepped mode calls step() instead."""
+    big, small = (8, 8, 8, 8), (4, 4, 4, 4)  # 16x fewer sites
+    srv = make_server([big, small], nslots=4, budget=10**9, engine_bytes=100)
+    assert srv.run_iters(big) == 8 and srv.run_iters(small) == 128
+    srv.run_cap = 64
+    assert srv.run_iters(small) == 64
+    reqs = [serving.Request(rid=0, volume=big, gauge=0, kappa=0.125, nrhs=2, kind="point", t_arrive=0.0),
+            serving.Request(rid=1, volume=small, gauge=0, kappa=0.125, nrhs=2, kind="point", t_arrive=0.0)]
+    done = srv.run(reqs, time_fn=FakeClock(1e-3))
+    assert len(done) == 2
+    caps = {tuple(sorted(set(e.run_caps))) for e in fake_engines.created}
+    assert caps == {(8,), (64,)}
+    srv.device_runs = False
+    srv.done = []
+    before = len(fake_engines.created)
+    reqs = [serving.Request(rid=2, volume=big, gauge=1, kappa=0.125, nrhs=1, kind="point", t_arrive=0.0)]
+    done = srv.run(reqs, time_fn=FakeClock(1e-3))
+    assert len(done) == 1
+    assert not hasattr(fake_engines.created[before], "run_caps")  # stepped, never run
+
