@@ -1168,6 +1168,7 @@ struct wl_engine {
   int loop_cap = 0;                // maxiter the loop graph was built for
   unsigned long long loop_gauge_id = 0;
   bool loop_failed = false;        // the loop graph could not be built: host-driven loop
+  const SolveLoop* capture_loop = nullptr;  // set while part 3 of a loop body is captured
   // engine run (wl_engine_run): WHILE node that stops when a slot finishes or at a per-launch cap
   cudaGraphExec_t grun = nullptr;
   int* run_state = nullptr;        // device: [0] cap, [1] active count at launch start, [2] iterations
@@ -1471,7 +1472,7 @@ static void enqueue_iteration(wl_engine* E, cudaStream_t st, int part) {
   }
   if (part == 3) {
     g_launches++;
-    cg_finalize_kernel<<<1, 128, 0, st>>>(Sc, n);
+    cg_finalize_kernel<<<1, 128, 0, st>>>(Sc, n, E->capture_loop ? *E->capture_loop : SolveLoop{});
     FUpdateP<SFS> f;  // p = rs + beta p
     sf2<S>(E->rs, f.rs);
     sf2<S>(E->p, f.p);
@@ -2104,8 +2105,8 @@ static wl_status engine_admit_all(wl_engine* E, const void* b, const void* x0, c
 
 // Appends one CG iteration to graph `g` (captured from stream st): part 1, the reliable-update
 // body (part 2) inside an IF node on a conditional handle created on g (the decide kernel of
-// part 1 sets it), then part 3 and, with `loop` set, the kernel that drives an enclosing WHILE
-// node.  Counts the unconditional kernels in *uncond and the body's in E->ru_body_kernels.
+// part 1 sets it), then part 3, whose finalize kernel also drives an enclosing WHILE node
+// when `loop` is set.  Counts the unconditional kernels in *uncond and the body's in E->ru_body_kernels.
 static cudaError_t capture_iteration(wl_engine* E, cudaStream_t st, cudaGraph_t g, const SolveLoop* loop,
                                      long long* uncond) {
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
@@ -2155,11 +2156,9 @@ static cudaError_t capture_iteration(wl_engine* E, cudaStream_t st, cudaGraph_t 
     e = cudaStreamBeginCaptureToGraph(st, g, &cond_node, nullptr, 1, mode);
     if (e == cudaSuccess) {
       const long long p3 = g_launches.load();
+      E->capture_loop = loop;  // the finalize kernel of part 3 drives the loop
       enqueue_part(E, st, 3);
-      if (loop) {
-        g_launches++;
-        solve_loop_kernel<<<1, 1, 0, st>>>(*loop);
-      }
+      E->capture_loop = nullptr;
       n_uncond += g_launches.load() - p3;
       cudaGraph_t g3 = nullptr;
       e = cudaStreamEndCapture(st, &g3);
@@ -2189,8 +2188,8 @@ static wl_status build_graph(wl_engine* E, cudaStream_t st) {
   return WL_OK;
 }
 
-// The whole solve as one graph: a WHILE node whose body is one iteration followed by
-// solve_loop_kernel, which keeps the loop going while any slot is active and fewer than
+// The whole solve as one graph: a WHILE node whose body is one iteration, whose finalize
+// kernel (solve_loop_step) keeps the loop going while any slot is active and fewer than
 // `cap` iterations have run (a hard bound on the device loop; slots stop at their maxiter
 // long before).  wl_solve launches it once per solve instead of launching an iteration graph
 // and synchronising on a status poll every check_every iterations.  On any failure the
@@ -2242,7 +2241,7 @@ static wl_status build_loop_graph(wl_engine* E, cudaStream_t st, bool run_mode =
 }
 
 // Up to max_iters iterations in one launch of the engine's run graph, stopping on the device
-// as soon as a slot finishes (see solve_loop_kernel); engines without graphs step instead.
+// as soon as a slot finishes (see solve_loop_step); engines without graphs step instead.
 extern "C" wl_status wl_engine_run(wl_engine* E, int max_iters) {
   NvtxRange nvtx_range("wl_engine_run");
   if (!E) WL_FAIL(nullptr, WL_ERR_ARG, "null engine");

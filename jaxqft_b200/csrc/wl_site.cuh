@@ -470,11 +470,12 @@ struct SolveLoop {
   int* total;           // engine run: iterations over all launches (else nullptr)
 };
 
-__global__ void solve_loop_kernel(SolveLoop L) {
+// One step of the loop: count the iteration and set the WHILE condition from the active
+// count `na` of this iteration.  Run by thread 0 of cg_finalize_kernel, which computes `na`.
+WL_D void solve_loop_step(const SolveLoop& L, int na) {
   const int c = *L.count + 1;
   *L.count = c;
   if (L.total) *L.total += 1;
-  const int na = *L.n_active;
   const int cap = L.capd ? *L.capd : L.cap;
   const bool more = na > 0 && c < cap && (L.start == nullptr || na >= *L.start);
   cudaGraphSetConditional(L.handle, more ? 1u : 0u);
@@ -487,7 +488,9 @@ __global__ void run_loop_setup_kernel(int* capd, int cap, int* start, const int*
   *count = 0;
 }
 
-__global__ void cg_finalize_kernel(CGScalars S, int n) {
+// With L.count set (an iteration captured inside a device-side loop) thread 0 also takes the
+// loop's step, so the loop costs no kernel of its own.
+__global__ void cg_finalize_kernel(CGScalars S, int n, SolveLoop L) {
   __shared__ int cnt;
   if (threadIdx.x == 0) cnt = 0;
   __syncthreads();
@@ -525,7 +528,10 @@ __global__ void cg_finalize_kernel(CGScalars S, int n) {
   }
   atomicAdd(&cnt, local);
   __syncthreads();
-  if (threadIdx.x == 0) *S.n_active = cnt;
+  if (threadIdx.x == 0) {
+    *S.n_active = cnt;
+    if (L.count) solve_loop_step(L, cnt);
+  }
 }
 
 }  // namespace wl

@@ -1,5 +1,5 @@
 """wl_solve runs a whole solve as one CUDA graph launch: a WHILE node around the captured
-CG iteration, continued by a one-thread kernel while any slot is active (and never more
+CG iteration, continued by its finalize kernel while any slot is active (and never more
 than the iteration limit plus a few).  wl_engine_run uses the same loop, stopping as soon
 as a slot finishes.  Their results must be the host-driven iteration's: the same kernels
 in the same order, so bitwise the same solutions, iteration counts and statuses, for
