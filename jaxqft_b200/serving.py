@@ -122,8 +122,8 @@ class PropagatorServer:
         self.nslots, self.inner, self.tol, self.maxiter = int(nslots), inner, float(tol), int(maxiter)
         self.iters_per_poll = int(iters_per_poll)
         self.run_cap = int(run_cap)
-        # False: drive the engines with iters_per_poll iterations per poll (wl_engine_step), as
-        # before device-side runs, for comparisons
+        # False: step each engine by iters_per_poll iterations per poll (wl_engine_step), for
+        # comparisons
         self.device_runs = bool(device_runs)
         # False: a finished request's device buffers (sources, right-hand sides, solutions) are
         # released as soon as it completes, as a server does once the response has been sent;
